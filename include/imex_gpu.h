@@ -1,0 +1,224 @@
+/*
+ * imex_gpu.h -- C ABI of the B200 (sm_100a) IMEX_SfloW2D time step.
+ *
+ * The reference (demichie/IMEX_SfloW2D_v2, Fortran 90 + OpenMP) has no FFI:
+ * its driver calls argument-less module routines that communicate through
+ * module globals.  This header is the drop-in boundary for those calls.  Each
+ * entry point names the reference routine it replaces:
+ *
+ *   imex_gpu_check_solve          <- check_solve(solve_all)      src/solver_2d.f90:666-857
+ *   imex_gpu_timestep             <- timestep                    src/solver_2d.f90:872-1005
+ *   imex_gpu_rk_step              <- imex_RK_solver              src/solver_2d.f90:1021-1632
+ *   imex_gpu_erosion_deposition   <- update_erosion_deposition_cell(dt)
+ *                                                                src/solver_2d.f90:2380-2595
+ *   imex_gpu_set_state/get_state  <- the module arrays q, qp     src/solver_2d.f90:68,157
+ *   imex_gpu_advance              <- one pass of the driver loop src/IMEX_SfloW2D.f90:337-389
+ *                                    (check_solve, timestep, dt clipping, imex_RK_solver,
+ *                                     update_erosion_deposition_cell, t = t + dt)
+ *
+ * All functions return an int status (IMEX_OK = 0).  Host arrays are owned by
+ * the caller and are only read or written during the call (synchronous).
+ * Layouts are the Fortran ones: q(n_vars,nx,ny) column-major, i.e. element
+ * (i,j,k) (0-based) at i + n_vars*(j + nx*k); cell planes (nx,ny) at j + nx*k;
+ * x-staggered planes (nx+1,ny) at j + (nx+1)*k; y-staggered (nx,ny+1) at j + nx*k.
+ * Cell indices reported back (first bad cell) are 1-based (j,k) as in Fortran.
+ *
+ * No function traps, asserts or spins without a bound on the device.
+ */
+#ifndef IMEX_GPU_H
+#define IMEX_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IMEX_MAX_SOLID 4
+#define IMEX_MAX_VARS (4 + IMEX_MAX_SOLID)
+#define IMEX_ABI_VERSION 1
+
+/* Status codes.  1..6 mirror the reference's fatal prints (which print and
+ * then block on READ(*,*) before continuing with the same values); the
+ * step is completed exactly as the reference completes it after the read. */
+enum {
+  IMEX_OK = 0,
+  IMEX_ENAN = 1,          /* NaN in q after the RK step     src/solver_2d.f90:1379 */
+  IMEX_ENEGH = 2,         /* h < -1e-7 after the RK step    src/solver_2d.f90:1405 */
+  IMEX_ENEGSOLID = 3,     /* solid <= -1e-7                 src/solver_2d.f90:1439 */
+  IMEX_ELOWT = 4,         /* T < 273 K                      src/solver_2d.f90:1538 */
+  IMEX_ESOLIDSUM = 5,     /* sum(solid) > q1 beyond 1e-10   src/solver_2d.f90:1569 */
+  IMEX_EEROSION = 6,      /* erosion/deposition checks      src/solver_2d.f90:2497,2520,2549 */
+  IMEX_ETIMEOUT = 7,      /* a bounded device wait gave up (never expected) */
+  IMEX_ECUDA = 8,         /* CUDA runtime error; see imex_gpu_last_error() */
+  IMEX_EINVAL = 9,        /* invalid argument / sizes */
+  IMEX_EUNSUPPORTED = 10, /* a reference option outside the implemented path */
+  IMEX_ENOMEM = 11,
+  IMEX_ENODEVICE = 12
+};
+
+/* Bits of ImexStats.error_mask (one per reference check). */
+#define IMEX_ERRBIT(code) (1u << (code))
+
+typedef struct ImexBC {
+  int32_t flag;   /* 0 Dirichlet, 1 Neumann (slope value), 2 one-sided slope */
+  int32_t pad_;
+  double value;
+} ImexBC;         /* TYPE bc, src/parameters_2d.f90:341-344 */
+
+/*
+ * Run parameters.  Field names follow the reference namelists
+ * (src/inpout_2d.f90:315-376) and module variables.  Derived constants
+ * (rho_a_amb, inv_pres, 1/rho_s, dx/2, 1/dx, eps_sing**4, the complex-step
+ * size n_vars*epsilon) are computed inside imex_gpu_create with the
+ * reference's formulas.
+ */
+typedef struct ImexParams {
+  int32_t abi_version;          /* must be IMEX_ABI_VERSION */
+  /* grid: src/geometry_2d.f90:185-300 */
+  int32_t nx, ny;               /* comp_cells_x, comp_cells_y */
+  int32_t n_solid;              /* 1..IMEX_MAX_SOLID; n_vars = 4 + n_solid */
+  double x0, y0, cell_size;
+  double eps_sing;              /* MIN(MIN(dx**4,dy**4),1e-10), geometry_2d.f90:286-290 */
+  /* numerics: NUMERIC_PARAMETERS */
+  int32_t n_rk;                 /* 2 (the only tableau with a non-trivial implicit stage used here) */
+  int32_t limiter[IMEX_MAX_VARS + 2]; /* limiter(1:n_vars+2); (n_vars+1,n_vars+2) = (2,3) */
+  double cfl, max_dt, reconstr_coeff, theta;
+  /* flags: NEWRUN_PARAMETERS etc. */
+  int32_t energy_flag, alpha_flag, gas_flag, liquid_flag;
+  int32_t rheology_flag, rheology_model;  /* models 0 (none), 1 Voellmy-Salm, 6 quadratic */
+  int32_t slope_correction_flag, curvature_term_flag;
+  int32_t radial_source_flag, lateral_source_flag, bottom_radial_source_flag;
+  int32_t settling_flag, entrainment_flag, erodible_deposit_flag, topo_change_flag;
+  int32_t pad_;
+  /* boundary conditions bcW/E/S/N(n_vars) */
+  ImexBC bcW[IMEX_MAX_VARS], bcE[IMEX_MAX_VARS], bcS[IMEX_MAX_VARS], bcN[IMEX_MAX_VARS];
+  /* physical constants: constitutive_2d.f90:33-262 */
+  double grav;
+  double T_ambient, pres, sp_heat_a, sp_gas_const_a, kin_visc_c;
+  double rho_s[IMEX_MAX_SOLID], diam_s[IMEX_MAX_SOLID], sp_heat_s[IMEX_MAX_SOLID];
+  double mu, xi, friction_factor;
+  double maximum_solid_packing;
+  /* radial / lateral inlet: RADIAL_SOURCE_PARAMETERS (after read_param's
+   * conversion of MFR/Ri into h_source, vel_source, alphas_source) */
+  double h_source, vel_source, T_source;
+  double alphas_source[IMEX_MAX_SOLID];
+  double time_param[4];
+  /* mass exchange: SOLID_TRANSPORT_PARAMETERS */
+  double erosion_coeff, erodible_porosity, T_erodible, alphastot_min;
+  double erodible_fract[IMEX_MAX_SOLID];
+  double rho_c_sub;             /* pres/(R_a*T_erodible), inpout_2d.f90:1733 */
+  double coeff_porosity;        /* erodible_porosity/(1-erodible_porosity), inpout_2d.f90:1683 */
+} ImexParams;
+
+/*
+ * Static per-run planes (host pointers, Fortran layout, copied at create).
+ * Required: B_prime_x_geom, B_prime_y_geom, solve_mask_time.
+ * grav_coeff, d_grav_coeff_dx, grav_coeff_stag_x/y: required when
+ *   slope_correction_flag; otherwise NULL (the reference sets them to 1 / 0).
+ * B_second_*_geom: required when curvature_term_flag, else NULL.
+ * source_cell/sourceE..N/source*_vect_*: required when radial_source_flag.
+ * B_cent, B_nodata: optional (NULL = zero / false).
+ * erodible, deposit, erosion: required when erosion_coeff>0 or settling_flag.
+ */
+typedef struct ImexStatic {
+  const double* B_cent;            /* (nx,ny) */
+  const double* B_prime_x_geom;    /* (nx,ny) */
+  const double* B_prime_y_geom;
+  const double* B_second_xx_geom;
+  const double* B_second_xy_geom;
+  const double* B_second_yy_geom;
+  const double* grav_coeff;
+  const double* d_grav_coeff_dx;
+  const double* grav_coeff_stag_x; /* (nx+1,ny) */
+  const double* grav_coeff_stag_y; /* (nx,ny+1) */
+  const int32_t* source_cell;      /* (nx,ny) 0 solved, 1 inlet interior, 2 inlet ring */
+  const int8_t* sourceE;
+  const int8_t* sourceW;
+  const int8_t* sourceS;
+  const int8_t* sourceN;
+  const double* sourceE_vect_x;
+  const double* sourceE_vect_y;
+  const double* sourceW_vect_x;
+  const double* sourceW_vect_y;
+  const double* sourceS_vect_x;
+  const double* sourceS_vect_y;
+  const double* sourceN_vect_x;
+  const double* sourceN_vect_y;
+  const int8_t* B_nodata;          /* (nx,ny) */
+  const double* solve_mask_time;   /* (nx,ny) release time per cell */
+  const double* erodible;          /* (n_solid,nx,ny) */
+  const double* deposit;           /* (nx,ny,n_solid) */
+  const double* erosion;           /* (nx,ny,n_solid) */
+} ImexStatic;
+
+typedef struct ImexStats {
+  int64_t solve_cells;             /* cells in solve_mask at the last check_solve */
+  int64_t newton_cells;            /* cells that entered solve_rk_step in the last step */
+  int64_t newton_iters;            /* sum of nl_iter at exit over those cells */
+  int64_t lnsrch_trials;           /* eval_f calls made by lnsrch */
+  int64_t newton_maxit_cells;      /* cells that used all max_nl_iter iterations */
+  int64_t newton_hist[16];         /* histogram of nl_iter (1..15, >=16 in the last bin) */
+  uint32_t error_mask;             /* OR of IMEX_ERRBIT(code) since the last stats read */
+  int32_t first_error_code;        /* code of the lowest-index offending cell (0 = none) */
+  int32_t first_error_j, first_error_k; /* 1-based cell of that code */
+  double dt;                       /* last dt used */
+  double t;                        /* model time held by the context */
+  int64_t steps;                   /* steps taken through imex_gpu_advance */
+  int64_t kernel_launches;         /* kernels launched by the context since create */
+} ImexStats;
+
+typedef struct ImexCtx ImexCtx;
+
+/* Context lifetime.  device < 0 selects the current CUDA device. */
+int imex_gpu_create(const ImexParams* p, const ImexStatic* s, int device, ImexCtx** out);
+int imex_gpu_destroy(ImexCtx* ctx);
+
+/* State transfer (host q in Fortran layout q(n_vars,nx,ny)). */
+int imex_gpu_set_state(ImexCtx* ctx, const double* q, double t);
+int imex_gpu_get_state(ImexCtx* ctx, double* q, double* qp /* (n_vars+2,nx,ny) or NULL */);
+/* Mass-exchange planes back to the host (any pointer may be NULL). */
+int imex_gpu_get_exchange(ImexCtx* ctx, double* erodible, double* deposit,
+                          double* erosion, double* B_cent);
+
+/* The reference's per-step routines, one call each. */
+int imex_gpu_check_solve(ImexCtx* ctx, double t, int solve_all, int64_t* n_solve_cells);
+int imex_gpu_timestep(ImexCtx* ctx, double* dt);
+int imex_gpu_rk_step(ImexCtx* ctx, double t, double dt);
+int imex_gpu_erosion_deposition(ImexCtx* ctx, double dt);
+
+/* Masks back to the host: solve_mask (nx,ny), solve_mask_x (nx+1,ny),
+ * solve_mask_y (nx,ny+1); 0/1 bytes.  Any pointer may be NULL. */
+int imex_gpu_get_masks(ImexCtx* ctx, int8_t* solve_mask, int8_t* mask_x, int8_t* mask_y);
+
+/*
+ * n_steps passes of the driver loop body (src/IMEX_SfloW2D.f90:339-389) with
+ * dt clipping on the device (no host round trip per step):
+ *   dt = min(dt_cfl, t_end - t, t_output - t, 1.1*0.5*(dt_old + dt_old_old)).
+ * dt_old/dt_old_old live in the context (initialised to dt0 by
+ * imex_gpu_set_clock).  t_output < 0 disables that clip.
+ * If use_graph != 0 the step sequence is captured once into a CUDA graph and
+ * replayed.  t (on return) is the model time after the last step.
+ */
+int imex_gpu_set_clock(ImexCtx* ctx, double t, double dt0, double t_end, double t_output);
+int imex_gpu_advance(ImexCtx* ctx, int n_steps, int use_graph, double* t);
+
+int imex_gpu_stats(ImexCtx* ctx, ImexStats* st, int reset_errors);
+const char* imex_gpu_last_error(ImexCtx* ctx);
+
+/* Synchronise the context stream (for host timing of asynchronous work). */
+int imex_gpu_sync(ImexCtx* ctx);
+
+/* Device-resident buffers for callers that bring their own device arrays
+ * (benchmarks): SoA planes q[v][k][pitch] of the context, and its pitch in
+ * elements.  The pointer stays valid for the context's life. */
+int imex_gpu_device_state(ImexCtx* ctx, double** q_dev, int64_t* pitch);
+
+/* Build information: "sm_100a fmad=0 ..." */
+const char* imex_gpu_build_info(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IMEX_GPU_H */

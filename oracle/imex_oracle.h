@@ -1,0 +1,73 @@
+/*
+ * imex_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * C API of the CPU oracle: a line-by-line C++ restatement of the reference
+ * IMEX_SfloW2D time step (src/solver_2d.f90, src/constitutive_2d.f90,
+ * src/geometry_2d.f90 limiters).  It exists to check the CUDA path; nothing
+ * in the product links or calls it.  Only tests/, __graft_entry__.smoke()
+ * and bench.py's cpu_baseline / reference arm load it.
+ *
+ * Parity status: the reference is Fortran and no Fortran compiler exists in
+ * this image, so the oracle could not be checked against the reference
+ * binary; the reference ships no golden outputs (TESTS/run_tests.sh only
+ * checks that output files exist).  Parity is therefore UNPINNED against the
+ * reference build; the oracle is pinned by analytic known-answer tests
+ * (lake at rest, mass conservation, symmetry, closed-form Voellmy relaxation,
+ * complex-step vs finite differences) in tests/test_oracle_*.py.
+ */
+#ifndef IMEX_ORACLE_H
+#define IMEX_ORACLE_H
+
+#include <stdint.h>
+#include "../include/imex_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct OracleCtx OracleCtx;
+
+OracleCtx* oracle_create(const ImexParams* p, const ImexStatic* s);
+void oracle_destroy(OracleCtx* o);
+/* q in Fortran layout; also runs check_solve(.TRUE.) and the initial qp sweep
+ * of the driver (src/IMEX_SfloW2D.f90:237-301). */
+void oracle_set_state(OracleCtx* o, const double* q, double t);
+void oracle_get_state(OracleCtx* o, double* q, double* qp);
+void oracle_get_exchange(OracleCtx* o, double* erodible, double* deposit,
+                         double* erosion, double* B_cent);
+int64_t oracle_check_solve(OracleCtx* o, double t, int solve_all);
+double oracle_timestep(OracleCtx* o);
+/* returns an error mask (IMEX_ERRBIT bits) of the reference's checks */
+uint32_t oracle_rk_step(OracleCtx* o, double t, double dt);
+uint32_t oracle_erosion_deposition(OracleCtx* o, double dt);
+void oracle_post_step(OracleCtx* o);
+void oracle_get_masks(OracleCtx* o, int8_t* m, int8_t* mx, int8_t* my);
+void oracle_set_clock(OracleCtx* o, double t, double dt0, double t_end, double t_output);
+/* n passes of the driver loop body; returns OR of error masks */
+uint32_t oracle_advance(OracleCtx* o, int n_steps, double* t);
+void oracle_stats(OracleCtx* o, ImexStats* st);
+/* reads of a neighbour's face or stage values that were written in an
+ * earlier step and belong to a cell that was wet then (the reference's
+ * arrays are never cleared between steps) */
+int64_t oracle_stale_wet_reads(OracleCtx* o);
+void oracle_set_threads(int n);
+int oracle_max_threads(void);
+
+/* Point functions exposed for unit tests (qc in, qp out; sizes n_vars / n_vars+2). */
+void oracle_qc_to_qp(OracleCtx* o, const double* qc, double* qp);
+void oracle_qp_to_qc(OracleCtx* o, const double* qp, double* qc);
+/* nh(1:n_vars) from eval_implicit_terms with complex input (re, im arrays) */
+void oracle_implicit_terms(OracleCtx* o, const double* q_re, const double* q_im,
+                           double* nh_re, double* nh_im);
+/* one solve_rk_step on a single cell: qj in/out, returns nl_iter at exit */
+int oracle_solve_rk_step(OracleCtx* o, double* qj, const double* qj_old,
+                         const double* rj_not_impl, double bprime_x,
+                         double bprime_y, double dt, double a_diag);
+double oracle_limit(double v1, double v2, double v3, double z1, double z2,
+                    double z3, int limiter, double theta);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,194 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes loader for the CPU oracle (liboracle.so).
+
+The oracle restates the reference Fortran time step on the CPU; tests and the
+benchmark's CPU baseline compare the CUDA path against it.  The product
+package never imports this module.  Parity is unpinned against the reference
+binary (no Fortran compiler in this image); see imex_oracle.h.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from imex_sflow2d_v2_b200.abi import ImexParams, ImexStatic, ImexStats, make_static
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def build(force=False):
+    so = os.path.join(_HERE, "liboracle.so")
+    src = os.path.join(_HERE, "imex_oracle.cpp")
+    if force or not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(src):
+        subprocess.check_call(["make", "-s", "-C", _HERE, "CXX=g++"])
+    return so
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        so = build()
+        L = C.CDLL(so)
+        vp = C.c_void_p
+        dp = C.POINTER(C.c_double)
+        L.oracle_create.restype = vp
+        L.oracle_create.argtypes = [C.POINTER(ImexParams), C.POINTER(ImexStatic)]
+        L.oracle_destroy.argtypes = [vp]
+        L.oracle_set_state.argtypes = [vp, dp, C.c_double]
+        L.oracle_get_state.argtypes = [vp, dp, dp]
+        L.oracle_get_exchange.argtypes = [vp, dp, dp, dp, dp]
+        L.oracle_check_solve.restype = C.c_int64
+        L.oracle_check_solve.argtypes = [vp, C.c_double, C.c_int]
+        L.oracle_timestep.restype = C.c_double
+        L.oracle_timestep.argtypes = [vp]
+        L.oracle_rk_step.restype = C.c_uint32
+        L.oracle_rk_step.argtypes = [vp, C.c_double, C.c_double]
+        L.oracle_erosion_deposition.restype = C.c_uint32
+        L.oracle_erosion_deposition.argtypes = [vp, C.c_double]
+        L.oracle_post_step.argtypes = [vp]
+        i8p = C.POINTER(C.c_int8)
+        L.oracle_get_masks.argtypes = [vp, i8p, i8p, i8p]
+        L.oracle_set_clock.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double]
+        L.oracle_advance.restype = C.c_uint32
+        L.oracle_advance.argtypes = [vp, C.c_int, dp]
+        L.oracle_stats.argtypes = [vp, C.POINTER(ImexStats)]
+        L.oracle_stale_wet_reads.restype = C.c_int64
+        L.oracle_stale_wet_reads.argtypes = [vp]
+        L.oracle_set_threads.argtypes = [C.c_int]
+        L.oracle_max_threads.restype = C.c_int
+        L.oracle_qc_to_qp.argtypes = [vp, dp, dp]
+        L.oracle_qp_to_qc.argtypes = [vp, dp, dp]
+        L.oracle_implicit_terms.argtypes = [vp, dp, dp, dp, dp]
+        L.oracle_solve_rk_step.restype = C.c_int
+        L.oracle_solve_rk_step.argtypes = [vp, dp, dp, dp, C.c_double, C.c_double,
+                                           C.c_double, C.c_double]
+        L.oracle_limit.restype = C.c_double
+        L.oracle_limit.argtypes = [C.c_double] * 6 + [C.c_int, C.c_double]
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Oracle:
+    """One oracle context; arrays use the Fortran layouts of imex_gpu.h."""
+
+    def __init__(self, params, static_arrays, threads=None):
+        L = lib()
+        if threads is not None:
+            L.oracle_set_threads(int(threads))
+        self.params = params
+        self.nx, self.ny, self.ns = params.nx, params.ny, params.n_solid
+        self.nv = 4 + self.ns
+        st, self._keep = make_static(static_arrays)
+        self._h = L.oracle_create(C.byref(params), C.byref(st))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().oracle_destroy(h)
+            self._h = None
+
+    def set_state(self, q, t=0.0):
+        q = np.ascontiguousarray(np.asarray(q, dtype=np.float64).ravel(order="F"))
+        lib().oracle_set_state(self._h, _p(q), float(t))
+
+    def get_state(self, with_qp=False):
+        q = np.zeros(self.nv * self.nx * self.ny)
+        qp = np.zeros((self.nv + 2) * self.nx * self.ny) if with_qp else None
+        lib().oracle_get_state(self._h, _p(q), _p(qp) if with_qp else None)
+        q = q.reshape((self.nv, self.nx, self.ny), order="F")
+        if with_qp:
+            return q, qp.reshape((self.nv + 2, self.nx, self.ny), order="F")
+        return q
+
+    def get_exchange(self):
+        n = self.nx * self.ny
+        er = np.zeros(self.ns * n)
+        de = np.zeros(self.ns * n)
+        eo = np.zeros(self.ns * n)
+        B = np.zeros(n)
+        lib().oracle_get_exchange(self._h, _p(er), _p(de), _p(eo), _p(B))
+        return (er.reshape((self.ns, self.nx, self.ny), order="F"),
+                de.reshape((self.nx, self.ny, self.ns), order="F"),
+                eo.reshape((self.nx, self.ny, self.ns), order="F"),
+                B.reshape((self.nx, self.ny), order="F"))
+
+    def check_solve(self, t, solve_all=False):
+        return lib().oracle_check_solve(self._h, float(t), int(solve_all))
+
+    def timestep(self):
+        return lib().oracle_timestep(self._h)
+
+    def rk_step(self, t, dt):
+        return lib().oracle_rk_step(self._h, float(t), float(dt))
+
+    def erosion_deposition(self, dt):
+        return lib().oracle_erosion_deposition(self._h, float(dt))
+
+    def post_step(self):
+        lib().oracle_post_step(self._h)
+
+    def get_masks(self):
+        nx, ny = self.nx, self.ny
+        m = np.zeros(nx * ny, np.int8)
+        mx = np.zeros((nx + 1) * ny, np.int8)
+        my = np.zeros(nx * (ny + 1), np.int8)
+        i8 = C.POINTER(C.c_int8)
+        lib().oracle_get_masks(self._h, m.ctypes.data_as(i8), mx.ctypes.data_as(i8),
+                               my.ctypes.data_as(i8))
+        return (m.reshape((nx, ny), order="F"), mx.reshape((nx + 1, ny), order="F"),
+                my.reshape((nx, ny + 1), order="F"))
+
+    def set_clock(self, t, dt0, t_end=1e300, t_output=-1.0):
+        lib().oracle_set_clock(self._h, float(t), float(dt0), float(t_end), float(t_output))
+
+    def advance(self, n_steps):
+        t = C.c_double(0.0)
+        err = lib().oracle_advance(self._h, int(n_steps), C.byref(t))
+        return err, t.value
+
+    def stats(self):
+        s = ImexStats()
+        lib().oracle_stats(self._h, C.byref(s))
+        return s
+
+    def stale_wet_reads(self):
+        return lib().oracle_stale_wet_reads(self._h)
+
+    # point functions
+    def qc_to_qp(self, qc):
+        qc = np.ascontiguousarray(qc, dtype=np.float64)
+        out = np.zeros(self.nv + 2)
+        lib().oracle_qc_to_qp(self._h, _p(qc), _p(out))
+        return out
+
+    def qp_to_qc(self, qp):
+        qp = np.ascontiguousarray(qp, dtype=np.float64)
+        out = np.zeros(self.nv)
+        lib().oracle_qp_to_qc(self._h, _p(qp), _p(out))
+        return out
+
+    def implicit_terms(self, q_re, q_im=None):
+        q_re = np.ascontiguousarray(q_re, dtype=np.float64)
+        q_im = None if q_im is None else np.ascontiguousarray(q_im, dtype=np.float64)
+        re = np.zeros(self.nv)
+        im = np.zeros(self.nv)
+        lib().oracle_implicit_terms(self._h, _p(q_re), _p(q_im) if q_im is not None else None,
+                                    _p(re), _p(im))
+        return re, im
+
+    def solve_rk_step(self, qj, qj_old, rj, bx, by, dt, a_diag=1.0):
+        qj = np.array(qj, dtype=np.float64)
+        qo = np.ascontiguousarray(qj_old, dtype=np.float64)
+        rj = np.ascontiguousarray(rj, dtype=np.float64)
+        it = lib().oracle_solve_rk_step(self._h, _p(qj), _p(qo), _p(rj), float(bx), float(by),
+                                        float(dt), float(a_diag))
+        return qj, it
+
+
+def limit(v1, v2, v3, z1, z2, z3, limiter, theta=1.0):
+    return lib().oracle_limit(v1, v2, v3, z1, z2, z3, int(limiter), float(theta))
