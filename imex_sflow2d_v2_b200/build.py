@@ -1,0 +1,37 @@
+"""Build libimexgpu.so for sm_100a (nvcc; no GPU needed)."""
+import os
+import subprocess
+import sys
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(_HERE, "csrc")
+LIB = os.path.join(_HERE, "libimexgpu.so")
+
+
+def sources():
+    return [os.path.join(CSRC, f) for f in ("imex_gpu.cu", "imex_kernels.cuh",
+                                             "imex_device.cuh")] + [
+        os.path.join(_HERE, "..", "include", "imex_gpu.h")]
+
+
+def needs_build():
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    return any(os.path.getmtime(s) > t for s in sources())
+
+
+def build(force=False, verbose=False):
+    if force or needs_build():
+        cmd = ["make", "-C", CSRC, "NVCC=/usr/local/cuda/bin/nvcc"]
+        if force:
+            cmd.insert(1, "-B")
+        out = subprocess.run(cmd, capture_output=not verbose, text=True)
+        if out.returncode != 0:
+            sys.stderr.write((out.stdout or "") + (out.stderr or ""))
+            raise RuntimeError("nvcc build of libimexgpu.so failed")
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

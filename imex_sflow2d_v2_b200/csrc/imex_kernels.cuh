@@ -1,0 +1,1261 @@
+// imex_kernels.cuh -- the per-step kernels of the IMEX_SfloW2D time step.
+//
+//   k_mask      check_solve: wet/source seed, n_RK=2 four-neighbour dilation in
+//               shared memory, inlet-interior removal (src/solver_2d.f90:666-857)
+//   k_flux      one tile per block: physical states of the tile and a 2-cell
+//               halo in shared memory, MUSCL faces with the reference's
+//               boundary/inlet rules, local speeds, Kurganov-Tadmor fluxes,
+//               divergence, explicit terms and the CFL minimum
+//               (timestep + RK stage 1: src/solver_2d.f90:872-1005,2614-3918)
+//   k_stage2    RK stage 2 per cell: semi-implicit terms, Newton with line
+//               search and complex-step Jacobian, assembly checks, optionally
+//               the erosion/deposition update (src/solver_2d.f90:1105-1628,
+//               1660-2365, 2380-2595)
+//
+// Data layout: structure-of-arrays planes, plane v of q at q + v*plane,
+// element (j,k) (0-based) at k*pitch + j.
+#pragma once
+
+#include "imex_device.cuh"
+
+namespace imex {
+
+constexpr int TX = 32;
+constexpr int TY = 8;
+constexpr int HALO = 2;
+constexpr int SW = TX + 2 * HALO;  // shared tile width
+constexpr int SH = TY + 2 * HALO;  // shared tile height
+constexpr int FLUX_THREADS = 288;
+constexpr int NXI = (TX + 1) * TY;  // x-interfaces per tile
+constexpr int NYI = TX * (TY + 1);  // y-interfaces per tile
+
+// Device clock shared by the step kernels (graph-replayable).
+struct DevClock {
+  double t, dt, dt_old, dt_old_old, t_end, t_output;
+  unsigned long long dtmin_bits;  // running CFL minimum (positive doubles)
+  unsigned int error_mask;
+  int pad_;
+  unsigned long long first_error;  // (cell index << 8) | code, min over cells
+  unsigned long long newton_cells, newton_iters, lnsrch_trials, newton_maxit;
+  unsigned long long hist[16];
+  unsigned long long solve_cells;
+  unsigned long long steps;
+};
+
+IMEX_HD double x_stag(const DevParams& P, int J) { return P.x0 + (double)(J - 1) * P.dx; }
+IMEX_HD double y_stag(const DevParams& P, int K) { return P.y0 + (double)(K - 1) * P.dy; }
+IMEX_HD double x_comp(const DevParams& P, int J) { return 0.5 * (x_stag(P, J) + x_stag(P, J + 1)); }
+IMEX_HD double y_comp(const DevParams& P, int K) { return 0.5 * (y_stag(P, K) + y_stag(P, K + 1)); }
+
+__device__ __forceinline__ void record_error(DevClock* clk, int code, long long cell) {
+  atomicOr(&clk->error_mask, 1u << code);
+  unsigned long long key = ((unsigned long long)cell << 8) | (unsigned long long)code;
+  atomicMin(&clk->first_error, key);
+}
+
+__device__ const RingCell* find_ring(const RingCell* ring, int n, long long idx) {
+  int lo = 0, hi = n - 1;
+  while (lo <= hi) {
+    int mid = (lo + hi) >> 1;
+    long long v = ring[mid].idx;
+    if (v == idx) return &ring[mid];
+    if (v < idx) lo = mid + 1; else hi = mid - 1;
+  }
+  return nullptr;
+}
+
+// ================================================================= k_mask
+// check_solve(.FALSE.) for n_RK = 2.
+__global__ void __launch_bounds__(256) k_mask(DevParams P, const double* __restrict__ q1,
+                                              const double* __restrict__ release_time,
+                                              const uint8_t* __restrict__ cellinfo,
+                                              const DevClock* clk, uint8_t* __restrict__ mask,
+                                              DevClock* clkw) {
+  __shared__ uint8_t s0[SH][SW];
+  __shared__ uint8_t s1[SH][SW];
+  const int j0 = blockIdx.x * TX, k0 = blockIdx.y * TY;
+  const double t = clk->t;
+  const int nx = P.nx, ny = P.ny;
+  for (int e = threadIdx.x; e < SW * SH; e += blockDim.x) {
+    int lx = e % SW, ly = e / SW;
+    int j = j0 + lx - HALO, k = k0 + ly - HALO;
+    uint8_t m = 0;
+    if (j >= 0 && j < nx && k >= 0 && k < ny) {
+      bool border = (j == 0 || j == nx - 1 || k == 0 || k == ny - 1);
+      if (border) {
+        m = 1;
+      } else {
+        size_t c = (size_t)k * P.pitch + j;
+        bool rel = P.has_release_time ? (release_time[c] <= t) : (0.0 <= t);
+        if (q1[c] > 0.0 && rel) m = 1;
+        if (P.radial_source_flag && (cellinfo[(size_t)k * nx + j] & CI_SRC_MASK) == 2) m = 1;
+      }
+    }
+    s0[ly][lx] = m;
+  }
+  __syncthreads();
+  // first dilation on the tile plus a 1-cell ring
+  for (int e = threadIdx.x; e < SW * SH; e += blockDim.x) {
+    int lx = e % SW, ly = e / SW;
+    int j = j0 + lx - HALO, k = k0 + ly - HALO;
+    uint8_t m = s0[ly][lx];
+    if (lx >= 1 && lx < SW - 1 && ly >= 1 && ly < SH - 1 && j >= 1 && j < nx - 1 && k >= 1 &&
+        k < ny - 1)
+      m = m | s0[ly][lx - 1] | s0[ly][lx + 1] | s0[ly - 1][lx] | s0[ly + 1][lx];
+    s1[ly][lx] = m;
+  }
+  __syncthreads();
+  int cnt = 0;
+  for (int e = threadIdx.x; e < TX * TY; e += blockDim.x) {
+    int lx = e % TX + HALO, ly = e / TX + HALO;
+    int j = j0 + lx - HALO, k = k0 + ly - HALO;
+    if (j >= nx || k >= ny) continue;
+    uint8_t m = s1[ly][lx];
+    if (j >= 1 && j < nx - 1 && k >= 1 && k < ny - 1)
+      m = m | s1[ly][lx - 1] | s1[ly][lx + 1] | s1[ly - 1][lx] | s1[ly + 1][lx];
+    if (P.radial_source_flag && (cellinfo[(size_t)k * nx + j] & CI_SRC_MASK) == 1) m = 0;
+    mask[(size_t)k * P.pitch + j] = m;
+    cnt += m;
+  }
+  // solve-cell count
+  for (int off = 16; off > 0; off >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, off);
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&clkw->solve_cells, (unsigned long long)cnt);
+}
+
+// ================================================================== faces
+// Shared tile of physical states: qps[v][ly][lx]; info_s[ly][lx] holds the
+// cellinfo bits plus bit 7 = solve mask.
+template <int NS>
+struct Tile {
+  double qp[6 + NS][SH][SW];
+  uint8_t info[SH][SW];
+};
+
+// Face states of one cell in one direction: W/E (dir 1) or S/N (dir 2).
+// `stage` selects the RK-stage arrays' view of never-solved inlet-interior
+// neighbours (all zero) instead of the module qp view (zero with T_ambient).
+template <int NS>
+__device__ void cell_faces(const DevParams& P, const Tile<NS>& T, int lx, int ly, int j, int k,
+                           int dir, bool stage, double time, const RingCell* ring,
+                           double* Fm, double* Fp) {
+  constexpr int NV = 4 + NS, NP = 6 + NS;
+  const uint8_t inf = T.info[ly][lx];
+  const int scell = inf & CI_SRC_MASK;
+  const bool rad = P.radial_source_flag != 0;
+  const bool sE = inf & CI_E, sW = inf & CI_W, sS = inf & CI_S, sN = inf & CI_N;
+  double sb[NP];
+#pragma unroll
+  for (int i = 0; i < NP; ++i) sb[i] = 0.0;
+  if (rad && scell == 2) {
+    const RingCell* rc = find_ring(ring, P.n_ring, (long long)k * P.nx + j);
+    if (rc) {
+      int w = sE ? 0 : (sW ? 1 : (sS ? 2 : 3));
+      eval_source_bdry<NS>(P, time, rc->vx[w], rc->vy[w], sb);
+    }
+  }
+  auto nb = [&](int v, int d) -> double {
+    int cx = (dir == 1) ? lx + d : lx;
+    int cy = (dir == 1) ? ly : ly + d;
+    if (stage && (T.info[cy][cx] & CI_SRC_MASK) == 1 && rad) return 0.0;
+    return T.qp[v][cy][cx];
+  };
+  const int J = j + 1, K = k + 1;  // Fortran indices
+  const int n = (dir == 1) ? P.nx : P.ny;
+  const int I = (dir == 1) ? J : K;
+  const double dh = (dir == 1) ? P.dx2 : P.dy2;
+  const double one_by_d = (dir == 1) ? P.one_by_dx : P.one_by_dy;
+  auto comp = [&](int m) { return (dir == 1) ? x_comp(P, m) : y_comp(P, m); };
+  auto stag = [&](int m) { return (dir == 1) ? x_stag(P, m) : y_stag(P, m); };
+  const int* flagm = (dir == 1) ? P.bcW_flag : P.bcS_flag;
+  const int* flagp = (dir == 1) ? P.bcE_flag : P.bcN_flag;
+  const double* valm = (dir == 1) ? P.bcW_val : P.bcS_val;
+  const double* valp = (dir == 1) ? P.bcE_val : P.bcN_val;
+  // inlet-ring corrections apply to the x direction through sE/sW and to the
+  // y direction through sS/sN; border inlet cells (lateral source) use the
+  // inlet state as the Dirichlet value in x only.
+  const bool ring_m = rad && scell == 2 && ((dir == 1) ? (!sE && sW) : (sS));
+  const bool ring_p = rad && scell == 2 && ((dir == 1) ? sE : (!sS && sN));
+  const bool border_src = (dir == 1) && scell == 2;
+  // stencil abscissae after the n_vars loop
+  double z1, z2 = comp(I), z3;
+  if (I == 1) {
+    z1 = stag(1);
+    z3 = comp(2);
+  } else if (I == n) {
+    z1 = comp(n - 1);
+    z3 = stag(n + 1);
+  } else {
+    z1 = ring_m ? stag(I) : comp(I - 1);
+    z3 = ring_p ? stag(I + 1) : comp(I + 1);
+  }
+  const double rc_d = P.reconstr_coeff * dh;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    double v2 = nb(i, 0), slope;
+    if (I == 1) {
+      if (border_src) {
+        slope = limit(sb[i], v2, nb(i, 1), z1, z2, z3, P.limiter[i], P.theta);
+      } else if (flagm[i] == 0) {
+        slope = limit(valm[i], v2, nb(i, 1), z1, z2, z3, P.limiter[i], P.theta);
+      } else if (flagm[i] == 1) {
+        slope = valm[i];
+      } else {
+        slope = (nb(i, 1) - nb(i, 0)) * one_by_d;
+      }
+    } else if (I == n) {
+      if (border_src) {
+        slope = limit(nb(i, -1), v2, sb[i], z1, z2, z3, P.limiter[i], P.theta);
+      } else if (flagp[i] == 0) {
+        slope = limit(nb(i, -1), v2, valp[i], z1, z2, z3, P.limiter[i], P.theta);
+      } else if (flagp[i] == 1) {
+        slope = valp[i];
+      } else {
+        slope = (nb(i, 0) - nb(i, -1)) * one_by_d;
+      }
+    } else {
+      double v1 = ring_m ? sb[i] : nb(i, -1);
+      double v3 = ring_p ? sb[i] : nb(i, 1);
+      slope = limit(v1, v2, v3, z1, z2, z3, P.limiter[i], P.theta);
+    }
+    double dq = rc_d * slope;
+    double fm = v2 - dq, fp = v2 + dq;
+    const int ivel = (dir == 1) ? 1 : 2;  // hu clamp in x, hv clamp in y
+    if (I == 1) {
+      if (border_src) fm = sb[i];
+      else if (flagm[i] == 0) fm = valm[i];
+      else if (i == ivel) fm = fmin_f(fm, 0.0);
+    }
+    if (I == n) {
+      if (border_src) fp = sb[i];
+      else if (flagp[i] == 0) fp = valp[i];
+      else if (i == ivel) fp = fmax_f(fp, 0.0);
+    }
+    Fm[i] = fm;
+    Fp[i] = fp;
+  }
+  // u and v with the limiters of hu and hv
+#pragma unroll
+  for (int a = 0; a < 2; ++a) {
+    const int i = NV + a;
+    double zz1 = z1, zz3 = z3;
+    if (dir == 1 && a == 1 && rad && scell == 2 && I > 1 && I < n && !sE && sN && !sS &&
+        K > 1 && K < P.ny)
+      zz3 = y_stag(P, K + 1);  // x_stencil(3)=y_stag(k+1), src/solver_2d.f90:3616
+    double v2 = nb(i, 0), v1, v3;
+    if (I == 1) {
+      v1 = (Fm[0] <= 0.0) ? 0.0 : Fm[1 + a] / Fm[0];
+      v3 = nb(i, 1);
+    } else if (I == n) {
+      v1 = nb(i, -1);
+      v3 = (Fp[0] <= 0.0) ? 0.0 : Fp[1 + a] / Fp[0];
+    } else {
+      v1 = ring_m ? sb[i] : nb(i, -1);
+      v3 = ring_p ? sb[i] : nb(i, 1);
+    }
+    double slope = limit(v1, v2, v3, zz1, z2, zz3, P.limiter[i], P.theta);
+    double dq = rc_d * slope;
+    Fm[i] = v2 - dq;
+    Fp[i] = v2 + dq;
+    if (I == 1) Fm[i] = v1;
+    else if (I == n) Fp[i] = v3;
+  }
+  if (I > 1 && I < n) {
+    if (ring_p) {
+#pragma unroll
+      for (int i = 0; i < NP; ++i) Fp[i] = sb[i];
+    } else if (ring_m) {
+#pragma unroll
+      for (int i = 0; i < NP; ++i) Fm[i] = sb[i];
+    }
+  }
+}
+
+// One interface: left/lower state from cell a, right/upper from cell b.
+// Writes the KT flux H (n_vars) and max(|a+|,|a-|) for the CFL.
+template <int NS>
+__device__ void interface_flux(const DevParams& P, const Tile<NS>& T, int dir, int la_x,
+                               int la_y, int ja, int ka, bool a_in, bool b_in, double gcf,
+                               bool stage, double time, const RingCell* ring, double* H,
+                               double& amax_flux, double& aneg_out, double& apos_out) {
+  constexpr int NV = 4 + NS, NP = 6 + NS;
+  const int lb_x = (dir == 1) ? la_x + 1 : la_x, lb_y = (dir == 1) ? la_y : la_y + 1;
+  const int jb = (dir == 1) ? ja + 1 : ja, kb = (dir == 1) ? ka : ka + 1;
+  double QL[NP], QR[NP], tmpm[NP], tmpp[NP];
+  const bool rad = P.radial_source_flag != 0;
+  const uint8_t ia = a_in ? T.info[la_y][la_x] : 0, ib = b_in ? T.info[lb_y][lb_x] : 0;
+  const bool a_int = rad && a_in && (ia & CI_SRC_MASK) == 1;
+  const bool b_int = rad && b_in && (ib & CI_SRC_MASK) == 1;
+  const uint8_t flag_b_m = (dir == 1) ? CI_W : CI_S;  // b's inlet lies on its minus side
+  const uint8_t flag_a_p = (dir == 1) ? CI_E : CI_N;
+  if (!a_in) {  // domain boundary on the minus side: both states from b's minus face
+    cell_faces<NS>(P, T, lb_x, lb_y, jb, kb, dir, stage, time, ring, QR, tmpp);
+#pragma unroll
+    for (int i = 0; i < NP; ++i) QL[i] = QR[i];
+  } else if (!b_in) {
+    cell_faces<NS>(P, T, la_x, la_y, ja, ka, dir, stage, time, ring, tmpm, QL);
+#pragma unroll
+    for (int i = 0; i < NP; ++i) QR[i] = QL[i];
+  } else {
+    bool have_a = false, have_b = false;
+    if (!a_int) {
+      cell_faces<NS>(P, T, la_x, la_y, ja, ka, dir, stage, time, ring, tmpm, QL);
+      have_a = true;
+    }
+    if (!b_int) {
+      cell_faces<NS>(P, T, lb_x, lb_y, jb, kb, dir, stage, time, ring, QR, tmpp);
+      have_b = true;
+    }
+    if (a_int) {
+      // never solved: only the ring copy of src/solver_2d.f90:3768-3771 fills it
+      bool copy = have_b && (ib & flag_b_m) && (ib & CI_SRC_MASK) == 2 &&
+                  ((dir == 1) ? !(ib & CI_E) : true);
+      if (dir == 2) copy = have_b && (ib & CI_S) && (ib & CI_SRC_MASK) == 2;
+#pragma unroll
+      for (int i = 0; i < NP; ++i) QL[i] = copy ? QR[i] : 0.0;
+    }
+    if (b_int) {
+      bool copy = have_a && (ia & flag_a_p) && (ia & CI_SRC_MASK) == 2;
+      if (dir == 2) copy = have_a && (ia & CI_N) && !(ia & CI_S) && (ia & CI_SRC_MASK) == 2;
+#pragma unroll
+      for (int i = 0; i < NP; ++i) QR[i] = copy ? QL[i] : 0.0;
+    }
+  }
+  double cL[NV], cR[NV];
+  qp_to_qc<NS>(P, QL, cL);
+  qp_to_qc<NS>(P, QR, cR);
+  Mixt mL = mixt_var<NS>(P, QL), mR = mixt_var<NS>(P, QR);
+  double lmin, lmax, rmin, rmax;
+  local_speeds<NS>(P, QL, mL, gcf, dir, lmin, lmax);
+  local_speeds<NS>(P, QR, mR, gcf, dir, rmin, rmax);
+  double aN = fmin_f(fmin_f(lmin, rmin), 0.0);
+  double aP = fmax_f(fmax_f(lmax, rmax), 0.0);
+  aneg_out = aN;
+  apos_out = aP;
+  amax_flux = fmax_f(aP, -aN);
+  double fL[NV], fR[NV];
+  eval_fluxes<NS>(P, cL, QL, mL, gcf, dir, fL);
+  eval_fluxes<NS>(P, cR, QR, mR, gcf, dir, fR);
+  if (aN == aP) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) H[i] = 0.0;
+  } else {
+    double coef = (aP * aN) / (aP - aN);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      double avg = (aP * fL[i] - aN * fR[i]) / (aP - aN);
+      H[i] = avg + coef * (cR[i] - cL[i]);
+    }
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int i = 0; i < NS; ++i) s += H[4 + i];
+  if (dir == 1) {
+    if (s / H[0] >= 1.0) {
+      double r = 0.0;
+#pragma unroll
+      for (int i = 0; i < NS; ++i) r += H[4 + i] / H[0];
+#pragma unroll
+      for (int i = 0; i < NS; ++i) H[4 + i] = H[4 + i] / r;
+    }
+    if (QL[1] == 0.0 && QR[1] == 0.0) {
+      H[0] = 0.0;
+#pragma unroll
+      for (int i = 3; i < NV; ++i) H[i] = 0.0;
+    }
+  } else {
+    if (s / H[0] > 1.0) {
+      double r = s / H[0];
+#pragma unroll
+      for (int i = 0; i < NS; ++i) H[4 + i] = H[4 + i] / r;
+    }
+    if (cL[2] == 0.0 && cR[2] == 0.0) {
+      H[0] = 0.0;
+#pragma unroll
+      for (int i = 3; i < NV; ++i) H[i] = 0.0;
+    }
+  }
+}
+
+// ================================================================= k_flux
+// Shared memory: Tile<NS> + Hx/Hy fluxes + per-interface CFL speeds.
+template <int NS>
+struct FluxShared {
+  Tile<NS> tile;
+  double Hx[4 + NS][TY][TX + 1];
+  double Hy[4 + NS][TY + 1][TX];
+  double ax[TY][TX + 1];
+  double ay[TY + 1][TX];
+  double dtmin[FLUX_THREADS / 32];
+};
+
+template <int NS>
+__global__ void __launch_bounds__(FLUX_THREADS)
+    k_flux(DevParams P, const double* __restrict__ q, const uint8_t* __restrict__ mask,
+           const uint8_t* __restrict__ cellinfo, const double* __restrict__ Bx,
+           const double* __restrict__ By, const double* __restrict__ Bxx,
+           const double* __restrict__ Bxy, const double* __restrict__ Byy,
+           const double* __restrict__ gc, const double* __restrict__ dgc,
+           const double* __restrict__ gcsx, const double* __restrict__ gcsy,
+           const RingCell* __restrict__ ring, DevClock* clk, double* __restrict__ X) {
+  constexpr int NV = 4 + NS, NP = 6 + NS;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FluxShared<NS>& S = *reinterpret_cast<FluxShared<NS>*>(smem_raw);
+  const int j0 = blockIdx.x * TX, k0 = blockIdx.y * TY;
+  const int nx = P.nx, ny = P.ny;
+  const double time = clk->t;
+  // any solve cell in the tile?
+  int any = 0;
+  for (int e = threadIdx.x; e < TX * TY; e += blockDim.x) {
+    int j = j0 + e % TX, k = k0 + e / TX;
+    if (j < nx && k < ny && mask[(size_t)k * P.pitch + j]) any = 1;
+  }
+  if (!__syncthreads_or(any)) return;
+  // physical states of the tile + halo
+  for (int e = threadIdx.x; e < SW * SH; e += blockDim.x) {
+    int lx = e % SW, ly = e / SW;
+    int j = j0 + lx - HALO, k = k0 + ly - HALO;
+    double qc[NV], qpv[NP];
+    uint8_t inf = 0;
+    if (j >= 0 && j < nx && k >= 0 && k < ny) {
+      size_t c = (size_t)k * P.pitch + j;
+      inf = P.has_cellinfo ? cellinfo[(size_t)k * nx + j] : 0;
+      if (mask[c]) inf |= 128;
+      if (P.radial_source_flag && (inf & CI_SRC_MASK) == 1) {
+        // inlet interior: never solved, holds its allocation value
+#pragma unroll
+        for (int i = 0; i < NP; ++i) qpv[i] = 0.0;
+        qpv[3] = P.T_ambient;
+      } else {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) qc[i] = q[c + (size_t)i * P.plane];
+        cell_qp<NS>(P, qc, qpv);
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < NP; ++i) qpv[i] = 0.0;
+    }
+#pragma unroll
+    for (int i = 0; i < NP; ++i) S.tile.qp[i][ly][lx] = qpv[i];
+    S.tile.info[ly][lx] = inf;
+  }
+  __syncthreads();
+  // interfaces
+  const RingCell* rg = ring;
+  for (int e = threadIdx.x; e < NXI + NYI; e += blockDim.x) {
+    int dir, ia_x, ia_y, ja, ka;
+    bool a_in, b_in;
+    double gcf;
+    if (e < NXI) {
+      dir = 1;
+      int jj = e % (TX + 1), kk = e / (TX + 1);
+      // interface between cells (j0+jj-1) and (j0+jj) in row k0+kk
+      ja = j0 + jj - 1;
+      ka = k0 + kk;
+      ia_x = jj - 1 + HALO;
+      ia_y = kk + HALO;
+      if (ka >= ny || ja + 1 > nx) { S.ax[kk][jj] = 0.0; continue; }
+      a_in = ja >= 0;
+      b_in = ja + 1 < nx;
+      bool sa = a_in && (S.tile.info[ia_y][ia_x] & 128);
+      bool sb_ = b_in && (S.tile.info[ia_y][ia_x + 1] & 128);
+      if (!(sa || sb_)) { S.ax[kk][jj] = 0.0; continue; }
+      gcf = P.slope_correction_flag ? gcsx[(size_t)ka * (nx + 1) + (ja + 1)] : 1.0;
+      double H[NV], amax, aN, aP;
+      interface_flux<NS>(P, S.tile, 1, ia_x, ia_y, ja, ka, a_in, b_in, gcf, true, time, rg, H,
+                         amax, aN, aP);
+      // CFL from the timestep view when an inlet-interior cell is in the stencil
+      bool dual = false;
+      if (P.radial_source_flag) {
+        for (int d = -1; d <= 2; ++d) {
+          int cx = ia_x + d;
+          int cj = ja + d;
+          if (cj >= 0 && cj < nx && (S.tile.info[ia_y][cx] & CI_SRC_MASK) == 1) dual = true;
+        }
+      }
+      if (dual) {
+        double H2[NV];
+        interface_flux<NS>(P, S.tile, 1, ia_x, ia_y, ja, ka, a_in, b_in, gcf, false, time, rg,
+                           H2, amax, aN, aP);
+      }
+#pragma unroll
+      for (int i = 0; i < NV; ++i) S.Hx[i][kk][jj] = H[i];
+      S.ax[kk][jj] = amax;
+    } else {
+      dir = 2;
+      int e2 = e - NXI;
+      int jj = e2 % TX, kk = e2 / TX;
+      ja = j0 + jj;
+      ka = k0 + kk - 1;
+      ia_x = jj + HALO;
+      ia_y = kk - 1 + HALO;
+      if (ja >= nx || ka + 1 > ny) { S.ay[kk][jj] = 0.0; continue; }
+      a_in = ka >= 0;
+      b_in = ka + 1 < ny;
+      bool sa = a_in && (S.tile.info[ia_y][ia_x] & 128);
+      bool sb_ = b_in && (S.tile.info[ia_y + 1][ia_x] & 128);
+      if (!(sa || sb_)) { S.ay[kk][jj] = 0.0; continue; }
+      gcf = P.slope_correction_flag ? gcsy[(size_t)(ka + 1) * nx + ja] : 1.0;
+      double H[NV], amax, aN, aP;
+      interface_flux<NS>(P, S.tile, 2, ia_x, ia_y, ja, ka, a_in, b_in, gcf, true, time, rg, H,
+                         amax, aN, aP);
+      bool dual = false;
+      if (P.radial_source_flag) {
+        for (int d = -1; d <= 2; ++d) {
+          int cy = ia_y + d;
+          int ck = ka + d;
+          if (ck >= 0 && ck < ny && (S.tile.info[cy][ia_x] & CI_SRC_MASK) == 1) dual = true;
+        }
+      }
+      if (dual) {
+        double H2[NV];
+        interface_flux<NS>(P, S.tile, 2, ia_x, ia_y, ja, ka, a_in, b_in, gcf, false, time, rg,
+                           H2, amax, aN, aP);
+      }
+#pragma unroll
+      for (int i = 0; i < NV; ++i) S.Hy[i][kk][jj] = H[i];
+      S.ay[kk][jj] = amax;
+    }
+  }
+  __syncthreads();
+  // cells: divergence, explicit terms, CFL
+  double dtl = P.max_dt;
+  for (int e = threadIdx.x; e < TX * TY; e += blockDim.x) {
+    int jj = e % TX, kk = e / TX;
+    int j = j0 + jj, k = k0 + kk;
+    if (j >= nx || k >= ny) continue;
+    int lx = jj + HALO, ly = kk + HALO;
+    if (!(S.tile.info[ly][lx] & 128)) continue;
+    size_t c = (size_t)k * P.pitch + j;
+    double qpv[NP], ex[NV];
+#pragma unroll
+    for (int i = 0; i < NP; ++i) qpv[i] = S.tile.qp[i][ly][lx];
+    double bx = Bx[c], by = By[c];
+    double bxx = 0.0, bxy = 0.0, byy = 0.0, gcf = 1.0, dg = 0.0;
+    if (P.curvature_term_flag) {
+      bxx = Bxx[c];
+      bxy = Bxy[c];
+      byy = Byy[c];
+    }
+    if (P.slope_correction_flag) {
+      gcf = gc[c];
+      dg = dgc[c];
+    }
+    eval_expl_terms<NS>(P, bx, by, bxx, bxy, byy, gcf, dg, qpv, ex);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      double d = 0.0;
+      d = d + (S.Hx[i][kk][jj + 1] - S.Hx[i][kk][jj]) * P.one_by_dx;
+      d = d + (S.Hy[i][kk + 1][jj] - S.Hy[i][kk][jj]) * P.one_by_dy;
+      X[c + (size_t)i * P.plane] = d - ex[i];
+    }
+    double max_a = fmax_f(S.ax[kk][jj], S.ax[kk][jj + 1]);
+    double dtx = (max_a > 0.0) ? P.cfl * P.dx / max_a : dtl;
+    max_a = fmax_f(S.ay[kk][jj], S.ay[kk + 1][jj]);
+    double dty = (max_a > 0.0) ? P.cfl * P.dy / max_a : dtl;
+    dtl = fmin_f(dtl, fmin_f(dtx, dty));
+  }
+  // block minimum, then a global atomic min on the bits of the positive double
+  for (int off = 16; off > 0; off >>= 1) dtl = fmin_f(dtl, __shfl_down_sync(0xffffffffu, dtl, off));
+  if ((threadIdx.x & 31) == 0) S.dtmin[threadIdx.x >> 5] = dtl;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = S.dtmin[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmin_f(m, S.dtmin[w]);
+    if (m > 0.0 && m < P.max_dt)
+      atomicMin(&clk->dtmin_bits, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+// =============================================================== Newton
+// solve_rk_step for a_diag = 1 (stage 2 of the n_RK = 2 tableau).
+template <int NS>
+struct NewtonOut {
+  int iters;
+  long long trials;
+};
+
+template <int NS>
+__device__ void eval_f(const DevParams& P, const double* qj, const double* qj_old,
+                       const double* Rj, double bx, double by, double dt, double* f,
+                       double& scal_f) {
+  constexpr int NV = 4 + NS;
+  double nh2, nh3;
+  implicit_terms_r<NS>(P, bx, by, qj, nh2, nh3);
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    double nh = (i == 1) ? nh2 : ((i == 2) ? nh3 : 0.0);
+    double R = Rj[i] - 1.0 * nh;
+    double fi = qj[i] - qj_old[i] + dt * R;
+    f[i] = 1.0 * fi;
+  }
+  double d = 0.0;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) d += f[i] * f[i];
+  scal_f = 0.5 * d;
+}
+
+template <int NS>
+__device__ NewtonOut<NS> solve_rk_step(const DevParams& P, double* qj, const double* qj_old,
+                                       const double* Rj, double bx, double by, double dt) {
+  constexpr int NV = 4 + NS;
+  const double TOLF = 1.0e-10, STPMX = 100.0;
+  double qj_org[NV], qj_rel[NV], rt[NV], x_old[NV], dd[NV];
+  double scal_f = 0.0;
+  long long trials = 0;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) qj_org[i] = fmax_f(fabs(qj[i]), 1.0e-3);
+#pragma unroll
+  for (int i = 0; i < NV; ++i) qj_rel[i] = qj[i] / qj_org[i];
+  int nl_iter;
+  for (nl_iter = 1; nl_iter <= 100; ++nl_iter) {
+    if (nl_iter == 1) {
+      eval_f<NS>(P, qj, qj_old, Rj, bx, by, dt, rt, scal_f);
+      double mx = fabs(rt[0]);
+#pragma unroll
+      for (int i = 1; i < NV; ++i) mx = fmax_f(mx, fabs(rt[i]));
+      if (mx < TOLF) break;
+    }
+    // Jacobian columns 2,3 by complex step (src/solver_2d.f90:2300-2365)
+    double J2[NV], J3[NV];  // left_matrix(:,2), left_matrix(:,3)
+#pragma unroll
+    for (int col = 1; col <= 2; ++col) {
+      cplx qc[NV];
+#pragma unroll
+      for (int m = 0; m < NV; ++m) qc[m] = mulr(C(qj_rel[m], (m == col) ? P.hstep : 0.0), qj_org[m]);
+      cplx nh2, nh3;
+      implicit_terms_c<NS>(P, bx, by, qc, nh2, nh3);
+      double* Lc = (col == 1) ? J2 : J3;
+#pragma unroll
+      for (int r = 0; r < NV; ++r) {
+        double nim = (r == 1) ? nh2.im : ((r == 2) ? nh3.im : 0.0);
+        double jac = 1.0 * nim * P.one_by_h;
+        double l0 = (r == col) ? 1.0 * qj_org[col] : 0.0;
+        Lc[r] = l0 - dt * 1.0 * jac;
+      }
+    }
+    // block elimination: explicit rows diagonal, 2x2 Cramer on rows/cols 2,3
+    double d1[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) d1[i] = (i == 1 || i == 2) ? 0.0 : rt[i] / (1.0 * qj_org[i]);
+    double d2a = rt[1], d2b = rt[2];
+    {
+      double s = 0.0, s2 = 0.0;
+#pragma unroll
+      for (int i = 0; i < NV; ++i)
+        if (i != 1 && i != 2) {
+          s += d1[i] * 0.0;
+        }
+#pragma unroll
+      for (int i = 0; i < NV; ++i)
+        if (i != 1 && i != 2) {
+          s2 += d1[i] * 0.0;
+        }
+      d2a = d2a - s;
+      d2b = d2b - s2;
+    }
+    double s11 = J2[1], s21 = J2[2], s12 = J3[1], s22 = J3[2];
+    double inv_det = 1.0 / (s11 * s22 - s21 * s12);
+    double sol0 = (d2a * s22 - d2b * s12) * inv_det;
+    double sol1 = (s11 * d2b - s21 * d2a) * inv_det;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      if (i == 1) dd[i] = -sol0 + 0.0;
+      else if (i == 2) dd[i] = -sol1 + 0.0;
+      else dd[i] = 0.0 + (-d1[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < NV; ++i) x_old[i] = qj_rel[i];
+    const double scal_f_old = scal_f;
+    if (nl_iter > 1) {
+      double sdot = 0.0;
+#pragma unroll
+      for (int i = 0; i < NV; ++i) sdot += qj_rel[i] * qj_rel[i];
+      double stpmax = STPMX * fmax_f(sqrt(sdot), (double)NV);
+      double grad[NV];
+#pragma unroll
+      for (int c = 0; c < NV; ++c) {
+        double s = 0.0;
+#pragma unroll
+        for (int r = 0; r < NV; ++r) {
+          double L;
+          if (c == 1) L = J2[r];
+          else if (c == 2) L = J3[r];
+          else L = (r == c) ? 1.0 * qj_org[c] : 0.0;
+          s += rt[r] * L;
+        }
+        grad[c] = s;
+      }
+      // lnsrch (src/solver_2d.f90:2019-2224)
+      double scale = 0.0, ssq = 0.0;
+#pragma unroll
+      for (int i = 0; i < NV; ++i) {
+        if (dd[i] != 0.0) {
+          double ax = fabs(dd[i]);
+          if (scale < ax) {
+            double val = scale / ax;
+            ssq = 1.0 + ssq * val * val;
+            scale = ax;
+          } else {
+            double val = ax / scale;
+            ssq = ssq + val * val;
+          }
+        }
+      }
+      double dabs = scale * sqrt(ssq);
+      if (dabs > stpmax) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) dd[i] = dd[i] * stpmax / dabs;
+      }
+      double slope = 0.0;
+#pragma unroll
+      for (int i = 0; i < NV; ++i) slope += grad[i] * dd[i];
+      double mx = 0.0;
+#pragma unroll
+      for (int i = 0; i < NV; ++i) {
+        double r = fabs(dd[i]) / fmax_f(fabs(x_old[i]), 1.0);
+        mx = (i == 0) ? r : fmax_f(mx, r);
+      }
+      double alamin = EPS / mx;
+      if (alamin == 0.0) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i];
+      } else {
+        double alam = 1.0;
+        // every backtrack after the first halves alam: the cubic model's
+        // value is clamped to <= alam/2 and then maxed with alam/2
+        for (int trial = 0; trial < 4096; ++trial) {
+          double qt[NV];
+#pragma unroll
+          for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i] + alam * dd[i];
+#pragma unroll
+          for (int i = 0; i < NV; ++i) qt[i] = qj_rel[i] * qj_org[i];
+          eval_f<NS>(P, qt, qj_old, Rj, bx, by, dt, rt, scal_f);
+          ++trials;
+          if (scal_f <= 0.9 * scal_f_old) break;
+          if (alam < alamin) {
+#pragma unroll
+            for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i];
+            scal_f = scal_f_old;
+            break;
+          }
+          if (alam == 1.0) {
+            double tmplam = -slope / (2.0 * (scal_f - scal_f_old - slope));
+            alam = fmax_f(tmplam, 0.5 * alam);
+          } else {
+            alam = 0.5 * alam;
+          }
+        }
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i] + dd[i];
+#pragma unroll
+      for (int i = 0; i < NV; ++i) qj[i] = qj_rel[i] * qj_org[i];
+      eval_f<NS>(P, qj, qj_old, Rj, bx, by, dt, rt, scal_f);
+    }
+#pragma unroll
+    for (int i = 0; i < NV; ++i) qj[i] = qj_rel[i] * qj_org[i];
+    double mx = fabs(rt[0]);
+#pragma unroll
+    for (int i = 1; i < NV; ++i) mx = fmax_f(mx, fabs(rt[i]));
+    if (mx < TOLF) break;
+    double m3 = 0.0;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      double r = fabs(qj_rel[i] - x_old[i]) / fmax_f(fabs(qj_rel[i]), 1.0);
+      m3 = (i == 0) ? r : fmax_f(m3, r);
+    }
+    if (m3 < EPS) break;
+  }
+  NewtonOut<NS> o;
+  o.iters = nl_iter > 100 ? 100 : nl_iter;
+  o.trials = trials;
+  return o;
+}
+
+// ============================================================ mass exchange
+template <int NS>
+__device__ void mass_exchange(const DevParams& P, const double* qpj, double bx, double by,
+                              const double* erod, double dtl, double* ers, double* dep,
+                              double& cpe, double& cpl, double* eqns, double& topo,
+                              bool& dep_neg) {
+  constexpr int NV = 4 + NS;
+#pragma unroll
+  for (int i = 0; i < NS; ++i) {
+    ers[i] = 0.0;
+    dep[i] = 0.0;
+  }
+  cpe = 0.0;
+  cpl = 0.0;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) eqns[i] = 0.0;
+  topo = 0.0;
+  if (qpj[0] <= EPS) return;
+  const double alpha_max = 0.6, hind_exp = 4.65;
+  double r_h = qpj[0], r_u = qpj[NV], r_v = qpj[NV + 1];
+  double al[NS];
+#pragma unroll
+  for (int i = 0; i < NS; ++i) al[i] = P.alpha_flag ? qpj[4 + i] : qpj[4 + i] / qpj[0];
+  double at = 0.0;
+#pragma unroll
+  for (int i = 0; i < NS; ++i) at += al[i];
+  double r_w = P.slope_correction_flag ? (r_u * bx + r_v * by) : 0.0;
+  double mv2 = r_u * r_u + r_v * r_v + r_w * r_w;
+  double mv = sqrt(mv2);
+  double tse;
+  if (P.erosion_coeff > 0.0) {
+    double te = P.erosion_coeff * mv * r_h * (1.0 - at);
+    tse = te * (1.0 - P.erodible_porosity);
+#pragma unroll
+    for (int i = 0; i < NS; ++i) ers[i] = P.erodible_fract[i] * tse;
+  }
+#pragma unroll
+  for (int i = 0; i < NS; ++i) ers[i] = fmax_f(0.0, fmin_f(ers[i], erod[i] / dtl));
+  tse = 0.0;
+#pragma unroll
+  for (int i = 0; i < NS; ++i) tse += ers[i];
+  double te = tse / (1.0 - P.erodible_porosity);
+  cpe = te * P.erodible_porosity;
+  if (at <= P.alphastot_min) return;
+  double r_T = qpj[3];
+  Mixt m = mixt_var<NS>(P, qpj);
+  double spc = sp_heat_c_of<NS>(P, qpj, m.rho_m);
+  double ikv = 1.0 / P.kin_visc_c;
+#pragma unroll
+  for (int i = 0; i < NS; ++i) {
+    if (al[i] > 0.0 && P.settling_flag) {
+      double sv = settling_velocity(P, P.diam_s[i], P.rho_s[i], m.rho_c, ikv);
+      dep[i] = al[i] * sv * 1.0;
+      dep[i] = dep[i] * pow(1.0 - fmin_f(1.0, at / alpha_max), hind_exp);
+      dep[i] = fmin_f(dep[i], r_h * al[i] / dtl);
+      if (dep[i] < 0.0) dep_neg = true;
+    }
+  }
+  double sdep = 0.0;
+#pragma unroll
+  for (int i = 0; i < NS; ++i) sdep += dep[i];
+  cpl = 0.0;
+  cpl = cpl + P.coeff_porosity * sdep;
+  double sal = 0.0;
+#pragma unroll
+  for (int i = 0; i < NS; ++i) sal += al[i];
+  cpl = fmin_f(cpl, r_h * fmax_f(0.0, P.maximum_solid_packing - sal) / dtl);
+  cpl = fmin_f(cpl, (r_h * (1.0 - sal) - P.coeff_porosity * (r_h * sal - dtl * sdep)) / dtl);
+  double T_erod = P.erodible_deposit_flag ? r_T : P.T_erodible;
+  double air_entr = 0.0;
+  if (P.entrainment_flag && r_h > 0.0 && m.Ri > 0.0) {
+    double entr_coeff = 0.075 / sqrt(1.0 + 718.0 * pow(m.Ri, 2.4));
+    air_entr = entr_coeff * sqrt(mv2);
+  }
+  double dep_tot = 0.0, ers_tot = 0.0, rdt = 0.0, ret = 0.0;
+#pragma unroll
+  for (int i = 0; i < NS; ++i) dep_tot += dep[i];
+#pragma unroll
+  for (int i = 0; i < NS; ++i) ers_tot += ers[i];
+#pragma unroll
+  for (int i = 0; i < NS; ++i) rdt += P.rho_s[i] * dep[i];
+#pragma unroll
+  for (int i = 0; i < NS; ++i) ret += P.rho_s[i] * ers[i];
+  eqns[0] = P.rho_a_amb * air_entr + ret - rdt + P.rho_c_sub * cpe - m.rho_c * cpl;
+  eqns[1] = -(r_u * (rdt + m.rho_c * cpl));
+  eqns[2] = -(r_v * (rdt + m.rho_c * cpl));
+  double sdh = 0.0, seh = 0.0;
+#pragma unroll
+  for (int i = 0; i < NS; ++i) sdh += P.rho_s[i] * P.sp_heat_s[i] * dep[i];
+#pragma unroll
+  for (int i = 0; i < NS; ++i) seh += P.rho_s[i] * P.sp_heat_s[i] * ers[i];
+  if (P.energy_flag)
+    eqns[3] = -(r_T * (sdh + m.rho_c * spc * cpl)) - 0.5 * mv2 * (rdt + m.rho_c * cpl) +
+              T_erod * (seh + P.rho_c_sub * spc * cpe) +
+              P.T_ambient * P.sp_heat_a * P.rho_a_amb * air_entr;
+  else
+    eqns[3] = -(r_T * (sdh + m.rho_c * spc * cpl)) + T_erod * (seh + P.rho_c_sub * spc * cpe) +
+              P.T_ambient * P.sp_heat_a * P.rho_a_amb * air_entr;
+#pragma unroll
+  for (int i = 0; i < NS; ++i) eqns[4 + i] = P.rho_s[i] * (ers[i] - dep[i]);
+  topo = (dep_tot - ers_tot) / (1.0 - P.erodible_porosity);
+}
+
+// update_erosion_deposition_cell for one cell (src/solver_2d.f90:2431-2588).
+template <int NS>
+__device__ bool erosion_cell(const DevParams& P, double* qc, double bx, double by,
+                             double* erod, double* depo, double* eros, double* Bc,
+                             double dtl) {
+  constexpr int NV = 4 + NS, NP = 6 + NS;
+  double qpv[NP];
+  cell_qp<NS>(P, qc, qpv);
+  double ers[NS], dep[NS], cpe, cpl, eqns[NV], topo;
+  bool bad = false;
+  mass_exchange<NS>(P, qpv, bx, by, erod, dtl, ers, dep, cpe, cpl, eqns, topo, bad);
+#pragma unroll
+  for (int i = 0; i < NV; ++i) qc[i] = qc[i] + dtl * eqns[i];
+#pragma unroll
+  for (int i = 0; i < NS; ++i) qc[4 + i] = fmax_f(0.0, qc[4 + i]);
+#pragma unroll
+  for (int i = 0; i < NS; ++i) depo[i] = depo[i] + dtl * dep[i];
+#pragma unroll
+  for (int i = 0; i < NS; ++i) eros[i] = eros[i] + dtl * ers[i];
+#pragma unroll
+  for (int i = 0; i < NS; ++i) erod[i] = erod[i] - dtl * ers[i];
+  if (P.erodible_deposit_flag) {
+#pragma unroll
+    for (int i = 0; i < NS; ++i) erod[i] = erod[i] + dtl * dep[i];
+  }
+  if (P.topo_change_flag) *Bc = *Bc + dtl * topo;
+#pragma unroll
+  for (int i = 0; i < NS; ++i) bad |= (qc[4 + i] < 0.0);
+  if (qc[0] <= 0.0) {
+    if (qc[0] > -1.0e-10) {
+#pragma unroll
+      for (int i = 0; i < NV; ++i) qc[i] = 0.0;
+    } else {
+      bad = true;
+    }
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int i = 0; i < NS; ++i) s += qc[4 + i];
+  if (s > qc[0]) {
+    if (qc[0] < 1.0e-10) {
+      double s2 = 0.0;
+#pragma unroll
+      for (int i = 0; i < NS; ++i) s2 += qc[4 + i];
+#pragma unroll
+      for (int i = 0; i < NS; ++i) qc[4 + i] = qc[4 + i] / s2 * qc[0];
+    } else {
+      bad = true;
+    }
+  }
+  double red_grav = 0.0;
+  if (qc[0] > 0.0) {
+    qc_to_qp<NS>(P, qc, qpv);
+    red_grav = mixt_var<NS>(P, qpv).red_grav;
+  }
+  if (red_grav <= 0.0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) qc[i] = 0.0;
+  }
+  return bad;
+}
+
+// =============================================================== k_stage2
+template <int NS, bool EROSION>
+__global__ void __launch_bounds__(128)
+    k_stage2(DevParams P, double* __restrict__ q, const double* __restrict__ X,
+             const uint8_t* __restrict__ mask, const uint8_t* __restrict__ cellinfo,
+             const double* __restrict__ Bx, const double* __restrict__ By,
+             const double* __restrict__ Bxx, const double* __restrict__ Bxy,
+             const double* __restrict__ Byy, const double* __restrict__ gc,
+             double* __restrict__ erodible, double* __restrict__ deposit,
+             double* __restrict__ erosion, double* __restrict__ Bcent, DevClock* clk) {
+  constexpr int NV = 4 + NS, NP = 6 + NS;
+  const int nx = P.nx, ny = P.ny;
+  const long long ncell = (long long)nx * ny;
+  long long newton_cells = 0, newton_iters = 0, trials = 0, maxit = 0;
+  const double dt = clk->dt;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < ncell;
+       g += (long long)gridDim.x * blockDim.x) {
+    int j = (int)(g % nx), k = (int)(g / nx);
+    size_t c = (size_t)k * P.pitch + j;
+    if (!mask[c]) continue;
+    double q0[NV], qfv[NV], Xc[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      q0[i] = q[c + (size_t)i * P.plane];
+      Xc[i] = X[c + (size_t)i * P.plane];
+    }
+    // q_fv = q0 - dt*(MATMUL(divFlux-expl, a_tilde) - MATMUL(NH+SI_NH, a_dirk))
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      double sa = (0.0 + Xc[i] * 1.0) + (0.0 - 0.0) * 0.0;
+      double sb = (0.0 + (0.0 + 0.0) * 0.0) + (0.0 + 0.0) * 0.0;
+      qfv[i] = q0[i] - dt * (sa - sb);
+    }
+    double qpv[NP];
+    qc_to_qp<NS>(P, qfv, qpv);
+    double qg[NV], qsi[NV];
+    const double bx = Bx[c], by = By[c];
+    if (qfv[0] > 0.0) {
+      double bxx = 0.0, bxy = 0.0, byy = 0.0, gcf = 1.0;
+      if (P.curvature_term_flag) {
+        bxx = Bxx[c];
+        bxy = Bxy[c];
+        byy = Byy[c];
+      }
+      if (P.slope_correction_flag) gcf = gc[c];
+      double si2, si3;
+      semi_impl_terms<NS>(P, bx, by, bxx, bxy, byy, gcf, qpv, si2, si3);
+      double SI[NV];
+#pragma unroll
+      for (int i = 0; i < NV; ++i) SI[i] = (i == 1) ? si2 : ((i == 2) ? si3 : 0.0);
+#pragma unroll
+      for (int i = 0; i < NV; ++i) qsi[i] = qfv[i] + dt * 1.0 * SI[i];
+      if (qfv[1] * qfv[1] + qfv[2] * qfv[2] == 0.0) {
+        qsi[1] = 0.0;
+        qsi[2] = 0.0;
+      } else if (qsi[1] * qfv[1] < 0.0 || qsi[2] * qfv[2] < 0.0) {
+        qsi[1] = 0.0;
+        qsi[2] = 0.0;
+      } else {
+        double Sm = sqrt(qsi[1] * qsi[1] + qsi[2] * qsi[2]);
+        double Fm = sqrt(qfv[1] * qfv[1] + qfv[2] * qfv[2]);
+        qsi[1] = Sm * qfv[1] / Fm;
+        qsi[2] = Sm * qfv[2] / Fm;
+      }
+      double Rj[NV];
+#pragma unroll
+      for (int i = 0; i < NV; ++i) {
+        SI[i] = (qsi[i] - qfv[i]) / (dt * 1.0);
+        double sa = 0.0 + Xc[i] * 1.0;
+        double sb = 0.0 + (0.0 + 0.0) * 0.0;
+        Rj[i] = (sa - sb) - 1.0 * SI[i];
+        qg[i] = qsi[i];
+      }
+      NewtonOut<NS> no = solve_rk_step<NS>(P, qg, q0, Rj, bx, by, dt);
+      newton_cells += 1;
+      newton_iters += no.iters;
+      trials += no.trials;
+      if (no.iters >= 100) maxit += 1;
+      atomicAdd(&clk->hist[no.iters < 16 ? no.iters - 1 : 15], 1ULL);
+      if (ny == 1) qg[2] = 0.0;
+      if (nx == 1) qg[1] = 0.0;
+      if (qsi[1] * qsi[1] + qsi[2] * qsi[2] == 0.0) {
+        qg[1] = 0.0;
+        qg[2] = 0.0;
+      } else if (qg[1] * qsi[1] <= 0.0 && qg[2] * qsi[2] <= 0.0) {
+        qg[1] = 0.0;
+        qg[2] = 0.0;
+      } else {
+        double Sm = sqrt(qg[1] * qg[1] + qg[2] * qg[2]);
+        double Fm = sqrt(qsi[1] * qsi[1] + qsi[2] * qsi[2]);
+        qg[1] = Sm * qsi[1] / Fm;
+        qg[2] = Sm * qsi[2] / Fm;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < NV; ++i) qg[i] = qfv[i];
+    }
+    // assemble_sol (src/solver_2d.f90:1339-1626)
+    double* qc = qg;
+    const long long cell = (long long)k * nx + j;
+    bool anynan = false;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) anynan |= isnan(qc[i]);
+    if (anynan) record_error(clk, 1, cell);
+    if (qc[0] < EPS) {
+      if (qc[0] > -1.0e-7) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) qc[i] = 0.0;
+      } else {
+        record_error(clk, 2, cell);
+      }
+    }
+    bool anyneg = false, anybad = false;
+#pragma unroll
+    for (int i = 0; i < NS; ++i) anyneg |= (qc[4 + i] < 0.0);
+    if (anyneg) {
+#pragma unroll
+      for (int i = 0; i < NS; ++i) anybad |= (qc[4 + i] <= -1.0e-7);
+      if (anybad) {
+        record_error(clk, 3, cell);
+      } else {
+#pragma unroll
+        for (int i = 0; i < NS; ++i)
+          if (qc[4 + i] > -1.0e-7) qc[4 + i] = 0.0;
+      }
+    }
+    qc_to_qp<NS>(P, qc, qpv);
+    if (qpv[3] < 273.0) record_error(clk, 4, cell);
+    double ssum = 0.0;
+#pragma unroll
+    for (int i = 0; i < NS; ++i) ssum += qc[4 + i];
+    if (ssum > qc[0]) {
+      if ((ssum - qc[0]) / qc[0] < 1.0e-10 || qc[0] < EPS) {
+        double s = 0.0;
+#pragma unroll
+        for (int i = 0; i < NS; ++i) s += qc[4 + i];
+#pragma unroll
+        for (int i = 0; i < NS; ++i) qc[4 + i] = qc[4 + i] / s * qc[0];
+      } else {
+        record_error(clk, 5, cell);
+      }
+    }
+    if (P.has_cellinfo && (cellinfo[cell] & CI_NODATA)) {
+#pragma unroll
+      for (int i = 0; i < NV; ++i) qc[i] = 0.0;
+    }
+    if (EROSION) {
+      double er[NS], de[NS], eo[NS], Bc = 0.0;
+      const size_t N = (size_t)P.plane;
+#pragma unroll
+      for (int i = 0; i < NS; ++i) {
+        er[i] = erodible[c + i * N];
+        de[i] = deposit[c + i * N];
+        eo[i] = erosion[c + i * N];
+      }
+      if (P.topo_change_flag) Bc = Bcent[c];
+      bool bad = erosion_cell<NS>(P, qc, bx, by, er, de, eo, &Bc, dt);
+#pragma unroll
+      for (int i = 0; i < NS; ++i) {
+        erodible[c + i * N] = er[i];
+        deposit[c + i * N] = de[i];
+        erosion[c + i * N] = eo[i];
+      }
+      if (P.topo_change_flag) Bcent[c] = Bc;
+      if (bad) record_error(clk, 6, cell);
+    }
+#pragma unroll
+    for (int i = 0; i < NV; ++i) q[c + (size_t)i * P.plane] = qc[i];
+  }
+  // counters
+  for (int off = 16; off > 0; off >>= 1) {
+    newton_cells += __shfl_down_sync(0xffffffffu, newton_cells, off);
+    newton_iters += __shfl_down_sync(0xffffffffu, newton_iters, off);
+    trials += __shfl_down_sync(0xffffffffu, trials, off);
+    maxit += __shfl_down_sync(0xffffffffu, maxit, off);
+  }
+  if ((threadIdx.x & 31) == 0 && newton_cells) {
+    atomicAdd(&clk->newton_cells, (unsigned long long)newton_cells);
+    atomicAdd(&clk->newton_iters, (unsigned long long)newton_iters);
+    atomicAdd(&clk->lnsrch_trials, (unsigned long long)trials);
+    atomicAdd(&clk->newton_maxit, (unsigned long long)maxit);
+  }
+}
+
+// Stand-alone erosion/deposition pass (imex_gpu_erosion_deposition).
+template <int NS>
+__global__ void __launch_bounds__(128)
+    k_erosion(DevParams P, double* __restrict__ q, const uint8_t* __restrict__ mask,
+              const double* __restrict__ Bx, const double* __restrict__ By,
+              double* __restrict__ erodible, double* __restrict__ deposit,
+              double* __restrict__ erosion, double* __restrict__ Bcent, DevClock* clk) {
+  constexpr int NV = 4 + NS;
+  const int nx = P.nx;
+  const long long ncell = (long long)nx * P.ny;
+  const double dt = clk->dt;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < ncell;
+       g += (long long)gridDim.x * blockDim.x) {
+    int j = (int)(g % nx), k = (int)(g / nx);
+    size_t c = (size_t)k * P.pitch + j;
+    if (!mask[c]) continue;
+    double qc[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) qc[i] = q[c + (size_t)i * P.plane];
+    double er[NS], de[NS], eo[NS], Bc = 0.0;
+    const size_t N = (size_t)P.plane;
+#pragma unroll
+    for (int i = 0; i < NS; ++i) {
+      er[i] = erodible[c + i * N];
+      de[i] = deposit[c + i * N];
+      eo[i] = erosion[c + i * N];
+    }
+    if (P.topo_change_flag) Bc = Bcent[c];
+    bool bad = erosion_cell<NS>(P, qc, Bx[c], By[c], er, de, eo, &Bc, dt);
+#pragma unroll
+    for (int i = 0; i < NS; ++i) {
+      erodible[c + i * N] = er[i];
+      deposit[c + i * N] = de[i];
+      erosion[c + i * N] = eo[i];
+    }
+    if (P.topo_change_flag) Bcent[c] = Bc;
+    if (bad) record_error(clk, 6, (long long)k * nx + j);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) q[c + (size_t)i * P.plane] = qc[i];
+  }
+}
+
+// ============================================================ small kernels
+// Resets the per-step accumulators of the clock.
+__global__ void k_step_begin(DevClock* clk, double max_dt, int reset_cells) {
+  clk->dtmin_bits = (unsigned long long)__double_as_longlong(max_dt);
+  if (reset_cells) clk->solve_cells = 0;
+  clk->newton_cells = 0;
+  clk->newton_iters = 0;
+  clk->lnsrch_trials = 0;
+  clk->newton_maxit = 0;
+  for (int b = 0; b < 16; ++b) clk->hist[b] = 0;
+}
+
+// dt from the CFL minimum with the driver's clipping (src/IMEX_SfloW2D.f90:359-381).
+__global__ void k_dt_clip(DevClock* clk, int clip) {
+  double dt = __longlong_as_double((long long)clk->dtmin_bits);
+  if (clip) {
+    double t = clk->t;
+    if (t + dt > clk->t_end) dt = clk->t_end - t;
+    if (clk->t_output >= 0.0 && t + dt > clk->t_output) dt = clk->t_output - t;
+    dt = fmin_f(dt, 1.1 * 0.5 * (clk->dt_old + clk->dt_old_old));
+    clk->dt_old_old = clk->dt_old;
+    clk->dt_old = dt;
+  }
+  clk->dt = dt;
+}
+
+__global__ void k_step_end(DevClock* clk) {
+  clk->t = clk->t + clk->dt;
+  clk->steps += 1;
+}
+
+// Fortran AoS q(n_vars,nx,ny) <-> SoA planes.
+__global__ void k_aos_to_soa(const double* __restrict__ aos, double* __restrict__ soa, int nv,
+                             int nx, int ny, long long pitch, long long plane) {
+  long long n = (long long)nx * ny;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < n * nv;
+       g += (long long)gridDim.x * blockDim.x) {
+    long long cell = g / nv;
+    int v = (int)(g % nv);
+    int j = (int)(cell % nx), k = (int)(cell / nx);
+    soa[(size_t)v * plane + (size_t)k * pitch + j] = aos[g];
+  }
+}
+__global__ void k_soa_to_aos(const double* __restrict__ soa, double* __restrict__ aos, int nv,
+                             int nx, int ny, long long pitch, long long plane) {
+  long long n = (long long)nx * ny;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < n * nv;
+       g += (long long)gridDim.x * blockDim.x) {
+    long long cell = g / nv;
+    int v = (int)(g % nv);
+    int j = (int)(cell % nx), k = (int)(cell / nx);
+    aos[g] = soa[(size_t)v * plane + (size_t)k * pitch + j];
+  }
+}
+
+// qp planes for imex_gpu_get_state (driver's post-step convention).
+template <int NS>
+__global__ void k_qp_out(DevParams P, const double* __restrict__ q, double* __restrict__ qp_aos,
+                         const uint8_t* __restrict__ cellinfo) {
+  constexpr int NV = 4 + NS, NP = 6 + NS;
+  long long n = (long long)P.nx * P.ny;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < n;
+       g += (long long)gridDim.x * blockDim.x) {
+    int j = (int)(g % P.nx), k = (int)(g / P.nx);
+    size_t c = (size_t)k * P.pitch + j;
+    double qc[NV], qpv[NP];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) qc[i] = q[c + (size_t)i * P.plane];
+    cell_qp<NS>(P, qc, qpv);
+#pragma unroll
+    for (int i = 0; i < NP; ++i) qp_aos[(size_t)g * NP + i] = qpv[i];
+  }
+}
+
+// solve_mask_x / solve_mask_y from solve_mask (src/solver_2d.f90:779-808).
+__global__ void k_masks_xy(DevParams P, const uint8_t* __restrict__ mask, int8_t* mx,
+                           int8_t* my) {
+  const int nx = P.nx, ny = P.ny;
+  long long nX = (long long)(nx + 1) * ny, nY = (long long)nx * (ny + 1);
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < nX + nY;
+       g += (long long)gridDim.x * blockDim.x) {
+    if (g < nX) {
+      int j = (int)(g % (nx + 1)), k = (int)(g / (nx + 1));
+      bool m = (j > 0 && mask[(size_t)k * P.pitch + j - 1]) || (j < nx && mask[(size_t)k * P.pitch + j]);
+      mx[g] = m ? 1 : 0;
+    } else {
+      long long h = g - nX;
+      int j = (int)(h % nx), k = (int)(h / nx);
+      bool m = (k > 0 && mask[(size_t)(k - 1) * P.pitch + j]) || (k < ny && mask[(size_t)k * P.pitch + j]);
+      my[h] = m ? 1 : 0;
+    }
+  }
+}
+
+}  // namespace imex

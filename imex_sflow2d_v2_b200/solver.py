@@ -1,0 +1,191 @@
+"""Host side of the B200 IMEX step: a thin ctypes layer over libimexgpu.so.
+
+The class mirrors the reference's per-step routines (src/solver_2d.f90):
+``check_solve`` (:666), ``timestep`` (:872), ``imex_RK_solver`` (:1021) and
+``update_erosion_deposition_cell`` (:2380), plus ``advance`` for whole driver
+loop passes (src/IMEX_SfloW2D.f90:337-389) executed on the device.  Arrays use
+the reference's Fortran layouts: q(n_vars, nx, ny), qp(n_vars+2, nx, ny).
+
+There is no CPU fallback: if the CUDA library cannot be loaded or no device
+is present, construction raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from .abi import (IMEX_OK, STATUS_NAMES, ImexParams, ImexStatic, ImexStats,
+                  make_static)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libimexgpu.so")
+_LIB = None
+
+
+class ImexError(RuntimeError):
+    def __init__(self, code, where, detail=""):
+        self.code = code
+        name = STATUS_NAMES.get(code, str(code))
+        super().__init__("%s failed: %s %s" % (where, name, detail))
+
+
+def load_library(path=LIB_PATH):
+    """Load libimexgpu.so (built by ``python -m imex_sflow2d_v2_b200.build``)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise RuntimeError("libimexgpu.so not found at %s: build it with "
+                           "`python -m imex_sflow2d_v2_b200.build`" % path)
+    L = C.CDLL(path)
+    vp = C.c_void_p
+    dp = C.POINTER(C.c_double)
+    i8p = C.POINTER(C.c_int8)
+    i64p = C.POINTER(C.c_int64)
+    sig = {
+        "imex_gpu_create": ([C.POINTER(ImexParams), C.POINTER(ImexStatic), C.c_int,
+                             C.POINTER(vp)], C.c_int),
+        "imex_gpu_destroy": ([vp], C.c_int),
+        "imex_gpu_set_state": ([vp, dp, C.c_double], C.c_int),
+        "imex_gpu_get_state": ([vp, dp, dp], C.c_int),
+        "imex_gpu_get_exchange": ([vp, dp, dp, dp, dp], C.c_int),
+        "imex_gpu_check_solve": ([vp, C.c_double, C.c_int, i64p], C.c_int),
+        "imex_gpu_timestep": ([vp, dp], C.c_int),
+        "imex_gpu_rk_step": ([vp, C.c_double, C.c_double], C.c_int),
+        "imex_gpu_erosion_deposition": ([vp, C.c_double], C.c_int),
+        "imex_gpu_get_masks": ([vp, i8p, i8p, i8p], C.c_int),
+        "imex_gpu_set_clock": ([vp, C.c_double, C.c_double, C.c_double, C.c_double], C.c_int),
+        "imex_gpu_advance": ([vp, C.c_int, C.c_int, dp], C.c_int),
+        "imex_gpu_stats": ([vp, C.POINTER(ImexStats), C.c_int], C.c_int),
+        "imex_gpu_last_error": ([vp], C.c_char_p),
+        "imex_gpu_sync": ([vp], C.c_int),
+        "imex_gpu_device_state": ([vp, C.POINTER(dp), i64p], C.c_int),
+        "imex_gpu_build_info": ([], C.c_char_p),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _LIB = L
+    return L
+
+
+def _p(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class ImexSolver:
+    """One device context holding the state of one run."""
+
+    def __init__(self, params, static_arrays, device=-1):
+        self.lib = load_library()
+        self.params = params
+        self.nx, self.ny, self.ns = params.nx, params.ny, params.n_solid
+        self.nv = 4 + self.ns
+        st, self._keep = make_static(static_arrays)
+        h = C.c_void_p()
+        rc = self.lib.imex_gpu_create(C.byref(params), C.byref(st), int(device), C.byref(h))
+        if rc != IMEX_OK:
+            raise ImexError(rc, "imex_gpu_create")
+        self._h = h
+
+    def _check(self, rc, where):
+        if rc != IMEX_OK and rc > 6:
+            raise ImexError(rc, where, self.lib.imex_gpu_last_error(self._h).decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.imex_gpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- state
+    def set_state(self, q, t=0.0):
+        q = np.ascontiguousarray(np.asarray(q, dtype=np.float64).ravel(order="F"))
+        return self._check(self.lib.imex_gpu_set_state(self._h, _p(q), float(t)), "set_state")
+
+    def get_state(self, with_qp=False):
+        n = self.nx * self.ny
+        q = np.zeros(self.nv * n)
+        qp = np.zeros((self.nv + 2) * n) if with_qp else None
+        self._check(self.lib.imex_gpu_get_state(self._h, _p(q), _p(qp) if with_qp else None),
+                    "get_state")
+        q = q.reshape((self.nv, self.nx, self.ny), order="F")
+        if with_qp:
+            return q, qp.reshape((self.nv + 2, self.nx, self.ny), order="F")
+        return q
+
+    def get_exchange(self):
+        n = self.nx * self.ny
+        er, de, eo, B = (np.zeros(self.ns * n), np.zeros(self.ns * n),
+                         np.zeros(self.ns * n), np.zeros(n))
+        self._check(self.lib.imex_gpu_get_exchange(self._h, _p(er), _p(de), _p(eo), _p(B)),
+                    "get_exchange")
+        return (er.reshape((self.ns, self.nx, self.ny), order="F"),
+                de.reshape((self.nx, self.ny, self.ns), order="F"),
+                eo.reshape((self.nx, self.ny, self.ns), order="F"),
+                B.reshape((self.nx, self.ny), order="F"))
+
+    # -- the reference's routines
+    def check_solve(self, t, solve_all=False):
+        n = C.c_int64(0)
+        self._check(self.lib.imex_gpu_check_solve(self._h, float(t), int(solve_all), C.byref(n)),
+                    "check_solve")
+        return n.value
+
+    def timestep(self):
+        dt = C.c_double(0.0)
+        self._check(self.lib.imex_gpu_timestep(self._h, C.byref(dt)), "timestep")
+        return dt.value
+
+    def imex_RK_solver(self, t, dt):
+        return self._check(self.lib.imex_gpu_rk_step(self._h, float(t), float(dt)), "rk_step")
+
+    def update_erosion_deposition_cell(self, dt):
+        return self._check(self.lib.imex_gpu_erosion_deposition(self._h, float(dt)),
+                           "erosion_deposition")
+
+    def get_masks(self):
+        nx, ny = self.nx, self.ny
+        m = np.zeros(nx * ny, np.int8)
+        mx = np.zeros((nx + 1) * ny, np.int8)
+        my = np.zeros(nx * (ny + 1), np.int8)
+        i8 = C.POINTER(C.c_int8)
+        self._check(self.lib.imex_gpu_get_masks(self._h, m.ctypes.data_as(i8),
+                                                mx.ctypes.data_as(i8), my.ctypes.data_as(i8)),
+                    "get_masks")
+        return (m.reshape((nx, ny), order="F"), mx.reshape((nx + 1, ny), order="F"),
+                my.reshape((nx, ny + 1), order="F"))
+
+    # -- driver loop on the device
+    def set_clock(self, t, dt0, t_end=1e300, t_output=-1.0):
+        return self._check(self.lib.imex_gpu_set_clock(self._h, float(t), float(dt0),
+                                                       float(t_end), float(t_output)),
+                           "set_clock")
+
+    def advance(self, n_steps, use_graph=False):
+        t = C.c_double(0.0)
+        rc = self._check(self.lib.imex_gpu_advance(self._h, int(n_steps), int(bool(use_graph)),
+                                                   C.byref(t)), "advance")
+        return rc, t.value
+
+    def stats(self, reset_errors=False):
+        s = ImexStats()
+        self._check(self.lib.imex_gpu_stats(self._h, C.byref(s), int(reset_errors)), "stats")
+        return s
+
+    def sync(self):
+        return self._check(self.lib.imex_gpu_sync(self._h), "sync")
+
+    def device_state(self):
+        p = C.POINTER(C.c_double)()
+        pitch = C.c_int64(0)
+        self._check(self.lib.imex_gpu_device_state(self._h, C.byref(p), C.byref(pitch)),
+                    "device_state")
+        return C.cast(p, C.c_void_p).value, pitch.value
