@@ -1,0 +1,325 @@
+#!/usr/bin/env python
+"""Throughput of the IMEX_SfloW2D time step on one B200 (or N independent
+replicas), printed as one JSON line.
+
+Workload: the 4096^2 synthetic fractal-DEM run (10 m cells, Hurst 0.8, 800 m
+relief + 15 degree slope, seeded; three solid classes 1e-5/1e-4/1e-3 m with
+settling and erosion; radial inlet 1e7 kg/s at 1000 K; Voellmy-Salm
+friction), with a 2 m resting current covering the DEM so that every cell
+carries the whole step (mask, MUSCL + KT fluxes, explicit terms, Newton
+relaxation, erosion/deposition).  A step = one pass of the driver loop
+(check_solve, timestep, dt clipping, imex_RK_solver,
+update_erosion_deposition_cell) on the device.
+
+  value     cell-updates/s with the state resident in HBM (CUDA events on
+            the stream the library runs on), summed over ranks
+  e2e       the same metric through the public API with host buffers: each
+            step uploads q from pinned host memory, advances, and reads q back
+  roofline  dominant kernel: algorithmic bytes per launch / its mean event time
+  cpu_baseline  the CPU oracle (a line-by-line C++ port of the reference,
+            OpenMP) on a 512^2 instance of the same workload generator
+
+`--impl reference` times that CPU port alone (the reference itself is
+Fortran and cannot be built here: no Fortran compiler in the image).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FP64 cell-updates/s (4096² grid); Newton iters/cell, learned vs plain"
+UNIT = "cell-updates/s"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=4096, help="grid side")
+    ap.add_argument("--layer", type=float, default=2.0, help="initial current thickness (m)")
+    ap.add_argument("--cpu-n", type=int, default=512, help="side of the CPU baseline sample")
+    ap.add_argument("--cpu-steps", type=int, default=0, help="0 = choose ~10-20 s of work")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n, layer):
+    from imex_sflow2d_v2_b200 import configs
+    return configs.fractal_inlet(n=n, initial_layer=layer)
+
+
+def bytes_per_cell(ns, erosion):
+    """Algorithmic bytes per cell and launch of each kernel (8-byte values)."""
+    nv = 4 + ns
+    mask = 8 + 1                                   # q1 read, mask byte written
+    flux = 8 * nv + 1 + 16 + 8 * nv                # q, mask, B'x, B'y read; X written
+    stage2 = 8 * nv + 8 * nv + 1 + 16 + 8 * nv     # q, X, mask, B' read; q written
+    if erosion:
+        stage2 += 2 * 3 * 8 * ns                   # erodible, deposit, erosion read+write
+    return {"mask": mask, "flux": flux, "stage2": stage2}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(args, threads=None):
+    """The CPU oracle on a bounded sample of the workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    orc.build()
+    p, st, q = workload(args.cpu_n, args.layer)
+    o = orc.Oracle(p, st, threads=threads)
+    o.set_state(q, 0.0)
+    o.set_clock(0.0, 1e-2)
+    o.advance(1)  # first step outside the timing (page-in)
+    steps = args.cpu_steps
+    if steps <= 0:
+        t0 = time.perf_counter()
+        o.advance(1)
+        one = time.perf_counter() - t0
+        steps = max(1, min(50, int(15.0 / max(one, 1e-3))))
+    t0 = time.perf_counter()
+    o.advance(steps)
+    el = time.perf_counter() - t0
+    cells = args.cpu_n * args.cpu_n
+    cores = orc.lib().oracle_max_threads() if threads is None else threads
+    return {"value": cells * steps / el, "unit": UNIT, "cores": int(cores), "kind": "port",
+            "sample": "%dx%d instance of the same generator (seed, physics, 2 m layer), "
+                      "%d steps after 2 untimed, %.1f s, OpenMP %d threads"
+                      % (args.cpu_n, args.cpu_n, steps, el, cores, )}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    cb = cpu_baseline(args)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "fractal-dem inlet, 3 solid classes, settling+erosion "
+                                   "(CPU sample %dx%d)" % (args.cpu_n, args.cpu_n),
+                       "grid": [args.cpu_n, args.cpu_n], "parallelism": "openmp"},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "note": "the reference is Fortran; no Fortran compiler in this image, so its "
+                    "C++ restatement (the oracle) is timed"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    from imex_sflow2d_v2_b200 import build as b
+    from imex_sflow2d_v2_b200.solver import ImexSolver, measure_fp64_peak
+    b.build()
+    p, st, q0 = workload(args.n, args.layer)
+    n = args.n
+    cells = n * n
+    g = ImexSolver(p, st, device=local)
+    stream = torch.cuda.current_stream()
+    g.set_stream(stream.cuda_stream)
+    g.set_state(q0, 0.0)
+    g.set_clock(0.0, 1e-2)
+    for _ in range(args.warmup):
+        g.advance(1)
+    g.sync()
+    s0 = g.stats(reset_errors=True)
+    g.profile(True)
+    sampler = ClockSampler(local)
+    sampler.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        g.advance(1)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    clocks = sampler.stop()
+    kt = g.kernel_times()
+    g.profile(False)
+    s1 = g.stats()
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        if dist:
+            dist.barrier()
+    value = world * cells * args.steps / (ms * 1e-3)
+    launches = int(s1.kernel_launches - s0.kernel_launches)
+    newton_per_cell = s1.newton_iters / max(1, s1.newton_cells)
+
+    # roofline of the dominant kernel (event times from the timed region)
+    erosion = bool(p.erosion_coeff != 0.0 or p.settling_flag)
+    bpc = bytes_per_cell(p.n_solid, erosion)
+    dom = max(kt, key=lambda k: kt[k][0])
+    dom_ms, dom_n = kt[dom]
+    avg_s = dom_ms / max(dom_n, 1) * 1e-3
+    alg_bytes = bpc[dom] * cells
+    peak = None
+    peak_src = "fallback"
+    try:
+        peak = float(json.load(open(PEAKS_FILE))["hbm_gbs"])
+        peak_src = "measured"
+    except Exception:
+        peak = FALLBACK_HBM_GBS
+    achieved = alg_bytes / avg_s / 1e9
+    traffic = None
+    try:
+        tr = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        traffic = tr.get(dom)
+    except Exception:
+        pass
+    fp64_peak = None
+    try:
+        fp64_peak = measure_fp64_peak(local)
+    except Exception:
+        pass
+
+    # end to end through the public API with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        nv = 4 + p.n_solid
+        hq = torch.empty(nv * cells, dtype=torch.float64, pin_memory=True).numpy()
+        hq[:] = np.asarray(q0).ravel(order="F")
+        g.set_clock(0.0, 1e-2)
+        g.sync()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            g.set_state(hq, 0.0)
+            g.advance(1)
+            g.get_state(out=hq)
+        g.sync()
+        el = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([el], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        e2e = {"value": world * cells * args.e2e_steps / el, "unit": UNIT,
+               "h2d_bytes_per_step": nv * cells * 8, "d2h_bytes_per_step": nv * cells * 8,
+               "steps": args.e2e_steps}
+
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(args)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "fractal-dem inlet %dx%d, 10 m cells, 3 solid classes, "
+                                   "settling+erosion, Voellmy, 2 m initial layer" % (n, n),
+                       "grid": [n, n], "cells": cells, "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (state %.2f GB)" % (8 * (4 + p.n_solid) * cells / 1e9),
+                       "solve_cells_per_step": int(s1.solve_cells)},
+            "newton_iters_per_cell": newton_per_cell,
+            "newton_cells_per_step": s1.newton_cells,
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
+                         "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
+                         "avg_launch_ms": avg_s * 1e3,
+                         "kernel_ms": {k: v[0] / max(v[1], 1) for k, v in kt.items()},
+                         "fp64_fma_peak_gflops": fp64_peak},
+            "e2e": e2e,
+            "cpu_baseline": cb,
+            "errors": int(s1.error_mask),
+        }
+        print(json.dumps(line), flush=True)
+    g.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

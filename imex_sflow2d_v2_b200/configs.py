@@ -126,10 +126,15 @@ def topography_geom(B, dx, dy):
     by = by / (10.0 * dy)
     bxx = bxx / (7.0 * dx ** 2)
     byy = byy / (7.0 * dy ** 2)
+    # the 25-point mixed stencil is the outer product of c1 with itself; it is
+    # applied as two 5-point passes (the sum order differs from the double
+    # loop of the reference only in the last bits)
+    tx = np.zeros((nx - 4, ny))
+    for kj in range(5):
+        tx = tx + c1[kj] * B[kj:kj + nx - 4, :]
     ws = np.zeros_like(bx)
     for kk in range(5):
-        for kj in range(5):
-            ws = ws + c1[kj] * c1[kk] * B[kj:kj + nx - 4, kk:kk + ny - 4]
+        ws = ws + c1[kk] * tx[:, kk:kk + ny - 4]
     bxy = ws / ((10.0 * dx) * (10.0 * dy))
     jj = np.clip(np.arange(nx), 2, nx - 3) - 2
     kk_ = np.clip(np.arange(ny), 2, ny - 3) - 2
@@ -409,12 +414,15 @@ def fractal_inlet(n=4096, dx=10.0, hurst=0.8, relief=800.0, slope_deg=15.0,
     static["erosion"] = np.zeros((n, n, ns), order="F")
     if initial_layer > 0.0:
         nv = 4 + ns
-        qp = np.zeros((nv + 2, n, n))
+        qp = np.zeros((nv + 2, 1, 1))
         qp[0] = initial_layer
         qp[3] = T_source
         for i in range(ns):
             qp[4 + i] = layer_alpha / ns * initial_layer
-        q = qp_to_qc_grid(p, qp)
+        cell = qp_to_qc_grid(p, qp)[:, 0, 0]   # the layer is uniform
+        q = np.empty((nv, n, n), order="F")
+        for i in range(nv):
+            q[i] = cell[i]
         q[:, static["source_cell"] == 1] = 0.0
     else:
         q = np.zeros((4 + ns, n, n), order="F")

@@ -23,6 +23,12 @@
 #ifndef IMEX_HD
 #define IMEX_HD __device__ __forceinline__
 #endif
+// Heavy point functions are kept out of line: they are called from several
+// places per kernel and inlining every copy multiplies code size (and ptxas
+// time) without a measurable gain for these FP64-bound bodies.
+#ifndef IMEX_NOINL
+#define IMEX_NOINL __device__ __noinline__
+#endif
 
 namespace imex {
 
@@ -186,7 +192,7 @@ IMEX_HD double sp_heat_c_of(const DevParams& P, const double* qpj, double rho_m)
 // ----------------------------------------------------------- qc_to_qp
 // r_phys_var + qc_to_qp; also returns red_grav through the out pointer.
 template <int NS>
-IMEX_HD void qc_to_qp(const DevParams& P, const double* qc, double* qp) {
+IMEX_NOINL void qc_to_qp(const DevParams& P, const double* qc, double* qp) {
   constexpr int NV = 4 + NS;
   if (!(qc[0] > EPS)) {
     qp[0] = 0.0;
@@ -280,7 +286,7 @@ IMEX_HD void cell_qp(const DevParams& P, const double* qc, double* qp) {
 
 // ----------------------------------------------------------- qp_to_qc
 template <int NS>
-IMEX_HD void qp_to_qc(const DevParams& P, const double* qp, double* qc) {
+IMEX_NOINL void qp_to_qc(const DevParams& P, const double* qp, double* qc) {
   constexpr int NV = 4 + NS;
   double r_h = qp[0];
   if (!(r_h > EPS)) {
@@ -336,8 +342,8 @@ IMEX_HD double maxmod(double a, double b) {
   double sa = a / fabs(a), sb = b / fabs(b);
   return 0.5 * (sa + sb) * fmax_f(fabs(a), fabs(b));
 }
-IMEX_HD double limit(double v1, double v2, double v3, double z1, double z2, double z3,
-                     int lim, double theta) {
+IMEX_NOINL double limit(double v1, double v2, double v3, double z1, double z2, double z3,
+                        int lim, double theta) {
   if (lim == 1) {
     // minmod(a,b) with a=(v3-v2)/(z3-z2), b=(v2-v1)/(z2-z1), z increasing:
     // when the two differences are finite and of opposite sign (or one is
@@ -556,8 +562,8 @@ IMEX_HD void implicit_terms_r(const DevParams& P, double bx, double by, const do
 
 // --------------------------------------------- implicit terms (complex)
 template <int NS>
-IMEX_HD void implicit_terms_c(const DevParams& P, double bx, double by, const cplx* q,
-                              cplx& nh2, cplx& nh3) {
+IMEX_NOINL void implicit_terms_c(const DevParams& P, double bx, double by, const cplx* q,
+                                 cplx& nh2, cplx& nh3) {
   nh2 = C(0.0, 0.0);
   nh3 = C(0.0, 0.0);
   if (!P.rheology_flag) return;
@@ -651,7 +657,7 @@ IMEX_HD void semi_impl_terms(const DevParams& P, double bx, double by, double bx
 }
 
 // ------------------------------------------------------ mass exchange
-IMEX_HD double settling_velocity(const DevParams& P, double diam, double rhos, double rhoc,
+IMEX_NOINL double settling_velocity(const DevParams& P, double diam, double rhos, double rhoc,
                                  double ikv) {
   double inv_sqrt_C_D = 1.0;
   if (rhos <= rhoc) return 0.0;

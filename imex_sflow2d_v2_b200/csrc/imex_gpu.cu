@@ -21,7 +21,9 @@ using namespace imex;
 struct ImexCtx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;  // created by the context
   DevParams P{};
+  DevParams* dP = nullptr;      // device copy of P
   ImexParams host_params{};
   int ns = 1;
   // device buffers
@@ -45,6 +47,11 @@ struct ImexCtx {
   int64_t launches = 0;
   uint32_t error_mask_acc = 0;
   std::string last_error;
+  // per-kernel CUDA-event timing (imex_gpu_profile)
+  bool prof = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;  // kernel id, events
+  size_t ev_used = 0;
 };
 
 namespace {
@@ -98,7 +105,7 @@ cudaError_t launch_flux_ns(ImexCtx* ctx) {
     attr_set = true;
   }
   k_flux<NS><<<tile_grid(P), FLUX_THREADS, smem, ctx->stream>>>(
-      P, ctx->q, ctx->mask, ctx->cellinfo, ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy, ctx->Byy,
+      ctx->dP, ctx->q, ctx->mask, ctx->cellinfo, ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy, ctx->Byy,
       ctx->gc, ctx->dgc, ctx->gcsx, ctx->gcsy, ctx->ring, ctx->clk, ctx->X);
   ctx->launches += 1;
   return cudaGetLastError();
@@ -117,7 +124,7 @@ template <int NS, bool ER>
 cudaError_t launch_stage2_ns(ImexCtx* ctx) {
   const DevParams& P = ctx->P;
   int grid = grid_1d((long long)P.nx * P.ny, 128);
-  k_stage2<NS, ER><<<grid, 128, 0, ctx->stream>>>(P, ctx->q, ctx->X, ctx->mask, ctx->cellinfo,
+  k_stage2<NS, ER><<<grid, 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->X, ctx->mask, ctx->cellinfo,
                                                   ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy, ctx->Byy,
                                                   ctx->gc, ctx->erodible, ctx->deposit,
                                                   ctx->erosion, ctx->Bcent, ctx->clk);
@@ -146,7 +153,7 @@ template <int NS>
 cudaError_t launch_erosion_ns(ImexCtx* ctx) {
   const DevParams& P = ctx->P;
   int grid = grid_1d((long long)P.nx * P.ny, 128);
-  k_erosion<NS><<<grid, 128, 0, ctx->stream>>>(P, ctx->q, ctx->mask, ctx->Bx, ctx->By,
+  k_erosion<NS><<<grid, 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->mask, ctx->Bx, ctx->By,
                                                ctx->erodible, ctx->deposit, ctx->erosion,
                                                ctx->Bcent, ctx->clk);
   ctx->launches += 1;
@@ -162,10 +169,10 @@ cudaError_t launch_erosion(ImexCtx* ctx) {
   }
 }
 
-cudaError_t launch_mask(ImexCtx* ctx) {
+cudaError_t launch_mask(ImexCtx* ctx, int solve_all = 0) {
   const DevParams& P = ctx->P;
-  k_mask<<<tile_grid(P), 256, 0, ctx->stream>>>(P, ctx->q, ctx->release, ctx->cellinfo,
-                                                ctx->clk, ctx->mask, ctx->clk);
+  k_mask<<<tile_grid(P), 256, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->release, ctx->cellinfo,
+                                                ctx->clk, ctx->mask, ctx->clk, solve_all);
   ctx->launches += 1;
   return cudaGetLastError();
 }
@@ -175,17 +182,57 @@ bool erosion_active(const ImexCtx* ctx) {
   return p.erosion_coeff != 0.0 || p.settling_flag || p.entrainment_flag;
 }
 
+// Kernel ids for imex_gpu_kernel_times.
+enum { KID_MASK = 0, KID_FLUX = 1, KID_STAGE2 = 2, KID_N = 3 };
+
+cudaEvent_t pool_event(ImexCtx* ctx) {
+  if (ctx->ev_used == ctx->ev_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    ctx->ev_pool.push_back(e);
+  }
+  return ctx->ev_pool[ctx->ev_used++];
+}
+
+struct ProfScope {
+  ImexCtx* ctx;
+  int kid;
+  cudaEvent_t a = nullptr, b = nullptr;
+  ProfScope(ImexCtx* c, int k) : ctx(c), kid(k) {
+    if (ctx->prof) {
+      a = pool_event(ctx);
+      b = pool_event(ctx);
+      cudaEventRecord(a, ctx->stream);
+    }
+  }
+  ~ProfScope() {
+    if (ctx->prof) {
+      cudaEventRecord(b, ctx->stream);
+      ctx->ev_pending.push_back({kid, {a, b}});
+    }
+  }
+};
+
 // Device part of one driver-loop pass: mask, fluxes + CFL, dt clip, stage 2
 // (+ erosion), t += dt.
 cudaError_t enqueue_step(ImexCtx* ctx) {
   cudaError_t e;
   k_step_begin<<<1, 1, 0, ctx->stream>>>(ctx->clk, ctx->P.max_dt, 1);
   ctx->launches += 1;
-  if ((e = launch_mask(ctx)) != cudaSuccess) return e;
-  if ((e = launch_flux(ctx)) != cudaSuccess) return e;
+  {
+    ProfScope ps(ctx, KID_MASK);
+    if ((e = launch_mask(ctx)) != cudaSuccess) return e;
+  }
+  {
+    ProfScope ps(ctx, KID_FLUX);
+    if ((e = launch_flux(ctx)) != cudaSuccess) return e;
+  }
   k_dt_clip<<<1, 1, 0, ctx->stream>>>(ctx->clk, 1);
   ctx->launches += 1;
-  if ((e = launch_stage2(ctx, erosion_active(ctx))) != cudaSuccess) return e;
+  {
+    ProfScope ps(ctx, KID_STAGE2);
+    if ((e = launch_stage2(ctx, erosion_active(ctx))) != cudaSuccess) return e;
+  }
   k_step_end<<<1, 1, 0, ctx->stream>>>(ctx->clk);
   ctx->launches += 1;
   return cudaGetLastError();
@@ -243,7 +290,8 @@ int imex_gpu_create(const ImexParams* p, const ImexStatic* s, int device, ImexCt
   } else {
     CK(cudaGetDevice(&ctx->device));
   }
-  CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking));
+  ctx->stream = ctx->own_stream;
   ctx->host_params = *p;
   ctx->ns = p->n_solid;
   DevParams& P = ctx->P;
@@ -441,6 +489,8 @@ int imex_gpu_create(const ImexParams* p, const ImexStatic* s, int device, ImexCt
     }
     CK(upload_plane(ctx, ctx->Bcent, s->B_cent, 0.0));
   }
+  CK(cudaMalloc((void**)&ctx->dP, sizeof(DevParams)));
+  CK(cudaMemcpy(ctx->dP, &ctx->P, sizeof(DevParams), cudaMemcpyHostToDevice));
   CK(cudaMalloc((void**)&ctx->clk, sizeof(DevClock)));
   CK(cudaMallocHost((void**)&ctx->clk_host, sizeof(DevClock)));
   std::memset(ctx->clk_host, 0, sizeof(DevClock));
@@ -464,11 +514,12 @@ int imex_gpu_destroy(ImexCtx* ctx) {
   if (ctx->graph) cudaGraphDestroy(ctx->graph);
   void* bufs[] = {ctx->q, ctx->X, ctx->mask, ctx->cellinfo, ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy,
                   ctx->Byy, ctx->gc, ctx->dgc, ctx->gcsx, ctx->gcsy, ctx->release, ctx->erodible,
-                  ctx->deposit, ctx->erosion, ctx->Bcent, ctx->ring, ctx->clk, ctx->scratch};
+                  ctx->deposit, ctx->erosion, ctx->Bcent, ctx->ring, ctx->clk, ctx->scratch, ctx->dP};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (ctx->clk_host) cudaFreeHost(ctx->clk_host);
-  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
   return IMEX_OK;
 }
@@ -511,10 +562,10 @@ int imex_gpu_get_state(ImexCtx* ctx, double* q, double* qp) {
   }
   if (qp) {
     switch (ctx->ns) {
-      case 1: k_qp_out<1><<<grid_1d((long long)N, 128), 128, 0, ctx->stream>>>(P, ctx->q, ctx->scratch, ctx->cellinfo); break;
-      case 2: k_qp_out<2><<<grid_1d((long long)N, 128), 128, 0, ctx->stream>>>(P, ctx->q, ctx->scratch, ctx->cellinfo); break;
-      case 3: k_qp_out<3><<<grid_1d((long long)N, 128), 128, 0, ctx->stream>>>(P, ctx->q, ctx->scratch, ctx->cellinfo); break;
-      default: k_qp_out<4><<<grid_1d((long long)N, 128), 128, 0, ctx->stream>>>(P, ctx->q, ctx->scratch, ctx->cellinfo); break;
+      case 1: k_qp_out<1><<<grid_1d((long long)N, 128), 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->scratch, ctx->cellinfo); break;
+      case 2: k_qp_out<2><<<grid_1d((long long)N, 128), 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->scratch, ctx->cellinfo); break;
+      case 3: k_qp_out<3><<<grid_1d((long long)N, 128), 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->scratch, ctx->cellinfo); break;
+      default: k_qp_out<4><<<grid_1d((long long)N, 128), 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->scratch, ctx->cellinfo); break;
     }
     ctx->launches += 1;
     CK(cudaGetLastError());
@@ -558,28 +609,7 @@ int imex_gpu_check_solve(ImexCtx* ctx, double t, int solve_all, int64_t* n_solve
   if (r) return r;
   const unsigned long long zero = 0;
   CK(cudaMemcpyAsync(&ctx->clk->solve_cells, &zero, sizeof(unsigned long long), cudaMemcpyHostToDevice, ctx->stream));
-  if (solve_all) {
-    // check_solve(.TRUE.): every cell except the inlet interior; the wet
-    // test adds nothing.  Emulated by a release time of -inf in a one-off
-    // mask: all interior cells seeded.
-    DevParams P2 = ctx->P;
-    std::vector<uint8_t> m((size_t)P2.plane, 0);
-    std::vector<uint8_t> info((size_t)P2.nx * P2.ny, 0);
-    if (P2.has_cellinfo)
-      CK(cudaMemcpy(info.data(), ctx->cellinfo, info.size(), cudaMemcpyDeviceToHost));
-    unsigned long long cnt = 0;
-    for (int k = 0; k < P2.ny; ++k)
-      for (int j = 0; j < P2.nx; ++j) {
-        uint8_t v = 1;
-        if (P2.radial_source_flag && (info[(size_t)k * P2.nx + j] & CI_SRC_MASK) == 1) v = 0;
-        m[(size_t)k * P2.pitch + j] = v;
-        cnt += v;
-      }
-    CK(cudaMemcpy(ctx->mask, m.data(), m.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(&ctx->clk->solve_cells, &cnt, sizeof(unsigned long long), cudaMemcpyHostToDevice));
-  } else {
-    CK(launch_mask(ctx));
-  }
+  CK(launch_mask(ctx, solve_all ? 1 : 0));
   ctx->x_valid = false;
   unsigned long long cnt = 0;
   CK(cudaMemcpyAsync(&cnt, &ctx->clk->solve_cells, sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
@@ -653,7 +683,7 @@ int imex_gpu_get_masks(ImexCtx* ctx, int8_t* solve_mask, int8_t* mask_x, int8_t*
   if (mask_x || mask_y) {
     size_t nX = (size_t)(nx + 1) * ny, nY = (size_t)nx * (ny + 1);
     int8_t* d = reinterpret_cast<int8_t*>(ctx->scratch);
-    k_masks_xy<<<grid_1d((long long)(nX + nY), 256), 256, 0, ctx->stream>>>(P, ctx->mask, d, d + nX);
+    k_masks_xy<<<grid_1d((long long)(nX + nY), 256), 256, 0, ctx->stream>>>(ctx->dP, ctx->mask, d, d + nX);
     ctx->launches += 1;
     CK(cudaGetLastError());
     if (mask_x) CK(cudaMemcpyAsync(mask_x, d, nX, cudaMemcpyDeviceToHost, ctx->stream));
@@ -750,6 +780,90 @@ int imex_gpu_sync(ImexCtx* ctx) {
   if (!ctx) return IMEX_EINVAL;
   CK(cudaSetDevice(ctx->device));
   CK(cudaStreamSynchronize(ctx->stream));
+  return IMEX_OK;
+}
+
+int imex_gpu_set_stream(ImexCtx* ctx, void* stream) {
+  if (!ctx) return IMEX_EINVAL;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->own_stream;
+  if (s != ctx->stream) {
+    // a captured graph is bound to nothing stream-specific, but keep the
+    // capture on the stream it will be replayed on
+    if (ctx->graph_exec) {
+      cudaGraphExecDestroy(ctx->graph_exec);
+      ctx->graph_exec = nullptr;
+    }
+    if (ctx->graph) {
+      cudaGraphDestroy(ctx->graph);
+      ctx->graph = nullptr;
+    }
+  }
+  ctx->stream = s;
+  return IMEX_OK;
+}
+
+int imex_gpu_profile(ImexCtx* ctx, int enable) {
+  if (!ctx) return IMEX_EINVAL;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->prof = enable != 0;
+  ctx->ev_pending.clear();
+  ctx->ev_used = 0;
+  return IMEX_OK;
+}
+
+int imex_gpu_kernel_times(ImexCtx* ctx, double* total_ms, int64_t* launches, int n_kernels) {
+  if (!ctx || !total_ms || !launches || n_kernels < KID_N) return IMEX_EINVAL;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < n_kernels; ++i) {
+    total_ms[i] = 0.0;
+    launches[i] = 0;
+  }
+  for (auto& pe : ctx->ev_pending) {
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, pe.second.first, pe.second.second));
+    total_ms[pe.first] += ms;
+    launches[pe.first] += 1;
+  }
+  ctx->ev_pending.clear();
+  ctx->ev_used = 0;
+  return IMEX_OK;
+}
+
+int imex_gpu_measure_fp64_peak(int device, double* gflops) {
+  ImexCtx* ctx = nullptr;
+  if (!gflops) return IMEX_EINVAL;
+  if (device >= 0) CK(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaGetDeviceProperties(&prop, dev));
+  double* out = nullptr;
+  CK(cudaMalloc((void**)&out, sizeof(double)));
+  const int threads = 256, blocks = prop.multiProcessorCount * 8, iters = 1 << 14;
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  k_fp64_probe<<<blocks, threads>>>(out, 64, 0.999999, 1e-7);
+  CK(cudaDeviceSynchronize());
+  float best = 1e30f;
+  for (int r = 0; r < 5; ++r) {
+    CK(cudaEventRecord(a));
+    k_fp64_probe<<<blocks, threads>>>(out, iters, 0.999999, 1e-7);
+    CK(cudaEventRecord(b));
+    CK(cudaEventSynchronize(b));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    best = std::min(best, ms);
+  }
+  double flops = 2.0 * 8.0 * iters * (double)threads * blocks;
+  *gflops = flops / (best * 1e-3) / 1e9;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(out);
   return IMEX_OK;
 }
 

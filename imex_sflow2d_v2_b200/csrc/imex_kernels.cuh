@@ -66,11 +66,12 @@ __device__ const RingCell* find_ring(const RingCell* ring, int n, long long idx)
 
 // ================================================================= k_mask
 // check_solve(.FALSE.) for n_RK = 2.
-__global__ void __launch_bounds__(256) k_mask(DevParams P, const double* __restrict__ q1,
+__global__ void __launch_bounds__(256) k_mask(const DevParams* __restrict__ Pp, const double* __restrict__ q1,
                                               const double* __restrict__ release_time,
                                               const uint8_t* __restrict__ cellinfo,
                                               const DevClock* clk, uint8_t* __restrict__ mask,
-                                              DevClock* clkw) {
+                                              DevClock* clkw, int solve_all) {
+  const DevParams& P = *Pp;
   __shared__ uint8_t s0[SH][SW];
   __shared__ uint8_t s1[SH][SW];
   const int j0 = blockIdx.x * TX, k0 = blockIdx.y * TY;
@@ -82,7 +83,7 @@ __global__ void __launch_bounds__(256) k_mask(DevParams P, const double* __restr
     uint8_t m = 0;
     if (j >= 0 && j < nx && k >= 0 && k < ny) {
       bool border = (j == 0 || j == nx - 1 || k == 0 || k == ny - 1);
-      if (border) {
+      if (border || solve_all) {
         m = 1;
       } else {
         size_t c = (size_t)k * P.pitch + j;
@@ -135,7 +136,7 @@ struct Tile {
 // `stage` selects the RK-stage arrays' view of never-solved inlet-interior
 // neighbours (all zero) instead of the module qp view (zero with T_ambient).
 template <int NS>
-__device__ void cell_faces(const DevParams& P, const Tile<NS>& T, int lx, int ly, int j, int k,
+__device__ __noinline__ void cell_faces(const DevParams& P, const Tile<NS>& T, int lx, int ly, int j, int k,
                            int dir, bool stage, double time, const RingCell* ring,
                            double* Fm, double* Fp) {
   constexpr int NV = 4 + NS, NP = 6 + NS;
@@ -390,13 +391,14 @@ struct FluxShared {
 
 template <int NS>
 __global__ void __launch_bounds__(FLUX_THREADS)
-    k_flux(DevParams P, const double* __restrict__ q, const uint8_t* __restrict__ mask,
+    k_flux(const DevParams* __restrict__ Pp, const double* __restrict__ q, const uint8_t* __restrict__ mask,
            const uint8_t* __restrict__ cellinfo, const double* __restrict__ Bx,
            const double* __restrict__ By, const double* __restrict__ Bxx,
            const double* __restrict__ Bxy, const double* __restrict__ Byy,
            const double* __restrict__ gc, const double* __restrict__ dgc,
            const double* __restrict__ gcsx, const double* __restrict__ gcsy,
            const RingCell* __restrict__ ring, DevClock* clk, double* __restrict__ X) {
+  const DevParams& P = *Pp;
   constexpr int NV = 4 + NS, NP = 6 + NS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   FluxShared<NS>& S = *reinterpret_cast<FluxShared<NS>*>(smem_raw);
@@ -575,7 +577,7 @@ struct NewtonOut {
 };
 
 template <int NS>
-__device__ void eval_f(const DevParams& P, const double* qj, const double* qj_old,
+__device__ __noinline__ void eval_f(const DevParams& P, const double* qj, const double* qj_old,
                        const double* Rj, double bx, double by, double dt, double* f,
                        double& scal_f) {
   constexpr int NV = 4 + NS;
@@ -617,7 +619,7 @@ __device__ NewtonOut<NS> solve_rk_step(const DevParams& P, double* qj, const dou
     }
     // Jacobian columns 2,3 by complex step (src/solver_2d.f90:2300-2365)
     double J2[NV], J3[NV];  // left_matrix(:,2), left_matrix(:,3)
-#pragma unroll
+#pragma unroll 1
     for (int col = 1; col <= 2; ++col) {
       cplx qc[NV];
 #pragma unroll
@@ -775,7 +777,7 @@ __device__ NewtonOut<NS> solve_rk_step(const DevParams& P, double* qj, const dou
 
 // ============================================================ mass exchange
 template <int NS>
-__device__ void mass_exchange(const DevParams& P, const double* qpj, double bx, double by,
+__device__ __noinline__ void mass_exchange(const DevParams& P, const double* qpj, double bx, double by,
                               const double* erod, double dtl, double* ers, double* dep,
                               double& cpe, double& cpl, double* eqns, double& topo,
                               bool& dep_neg) {
@@ -941,13 +943,14 @@ __device__ bool erosion_cell(const DevParams& P, double* qc, double bx, double b
 // =============================================================== k_stage2
 template <int NS, bool EROSION>
 __global__ void __launch_bounds__(128)
-    k_stage2(DevParams P, double* __restrict__ q, const double* __restrict__ X,
+    k_stage2(const DevParams* __restrict__ Pp, double* __restrict__ q, const double* __restrict__ X,
              const uint8_t* __restrict__ mask, const uint8_t* __restrict__ cellinfo,
              const double* __restrict__ Bx, const double* __restrict__ By,
              const double* __restrict__ Bxx, const double* __restrict__ Bxy,
              const double* __restrict__ Byy, const double* __restrict__ gc,
              double* __restrict__ erodible, double* __restrict__ deposit,
              double* __restrict__ erosion, double* __restrict__ Bcent, DevClock* clk) {
+  const DevParams& P = *Pp;
   constexpr int NV = 4 + NS, NP = 6 + NS;
   const int nx = P.nx, ny = P.ny;
   const long long ncell = (long long)nx * ny;
@@ -1125,10 +1128,11 @@ __global__ void __launch_bounds__(128)
 // Stand-alone erosion/deposition pass (imex_gpu_erosion_deposition).
 template <int NS>
 __global__ void __launch_bounds__(128)
-    k_erosion(DevParams P, double* __restrict__ q, const uint8_t* __restrict__ mask,
+    k_erosion(const DevParams* __restrict__ Pp, double* __restrict__ q, const uint8_t* __restrict__ mask,
               const double* __restrict__ Bx, const double* __restrict__ By,
               double* __restrict__ erodible, double* __restrict__ deposit,
               double* __restrict__ erosion, double* __restrict__ Bcent, DevClock* clk) {
+  const DevParams& P = *Pp;
   constexpr int NV = 4 + NS;
   const int nx = P.nx;
   const long long ncell = (long long)nx * P.ny;
@@ -1165,6 +1169,19 @@ __global__ void __launch_bounds__(128)
 }
 
 // ============================================================ small kernels
+// FMA-chain throughput probe: each thread runs 8 independent chains of
+// `iters` dependent fused multiply-adds (the measured FP64 peak).
+__global__ void k_fp64_probe(double* out, int iters, double a, double b) {
+  double x0 = threadIdx.x * 1e-9, x1 = x0 + 1.0, x2 = x0 + 2.0, x3 = x0 + 3.0;
+  double x4 = x0 + 4.0, x5 = x0 + 5.0, x6 = x0 + 6.0, x7 = x0 + 7.0;
+  for (int i = 0; i < iters; ++i) {
+    x0 = __fma_rn(x0, a, b); x1 = __fma_rn(x1, a, b); x2 = __fma_rn(x2, a, b); x3 = __fma_rn(x3, a, b);
+    x4 = __fma_rn(x4, a, b); x5 = __fma_rn(x5, a, b); x6 = __fma_rn(x6, a, b); x7 = __fma_rn(x7, a, b);
+  }
+  double r = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (r == 12345.678) out[0] = r;  // keeps the chains live
+}
+
 // Resets the per-step accumulators of the clock.
 __global__ void k_step_begin(DevClock* clk, double max_dt, int reset_cells) {
   clk->dtmin_bits = (unsigned long long)__double_as_longlong(max_dt);
@@ -1221,8 +1238,9 @@ __global__ void k_soa_to_aos(const double* __restrict__ soa, double* __restrict_
 
 // qp planes for imex_gpu_get_state (driver's post-step convention).
 template <int NS>
-__global__ void k_qp_out(DevParams P, const double* __restrict__ q, double* __restrict__ qp_aos,
+__global__ void k_qp_out(const DevParams* __restrict__ Pp, const double* __restrict__ q, double* __restrict__ qp_aos,
                          const uint8_t* __restrict__ cellinfo) {
+  const DevParams& P = *Pp;
   constexpr int NV = 4 + NS, NP = 6 + NS;
   long long n = (long long)P.nx * P.ny;
   for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < n;
@@ -1239,8 +1257,9 @@ __global__ void k_qp_out(DevParams P, const double* __restrict__ q, double* __re
 }
 
 // solve_mask_x / solve_mask_y from solve_mask (src/solver_2d.f90:779-808).
-__global__ void k_masks_xy(DevParams P, const uint8_t* __restrict__ mask, int8_t* mx,
+__global__ void k_masks_xy(const DevParams* __restrict__ Pp, const uint8_t* __restrict__ mask, int8_t* mx,
                            int8_t* my) {
+  const DevParams& P = *Pp;
   const int nx = P.nx, ny = P.ny;
   long long nX = (long long)(nx + 1) * ny, nY = (long long)nx * (ny + 1);
   for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < nX + nY;

@@ -60,6 +60,10 @@ def load_library(path=LIB_PATH):
         "imex_gpu_last_error": ([vp], C.c_char_p),
         "imex_gpu_sync": ([vp], C.c_int),
         "imex_gpu_device_state": ([vp, C.POINTER(dp), i64p], C.c_int),
+        "imex_gpu_set_stream": ([vp, vp], C.c_int),
+        "imex_gpu_profile": ([vp, C.c_int], C.c_int),
+        "imex_gpu_kernel_times": ([vp, dp, i64p, C.c_int], C.c_int),
+        "imex_gpu_measure_fp64_peak": ([C.c_int, dp], C.c_int),
         "imex_gpu_build_info": ([], C.c_char_p),
     }
     for name, (args, res) in sig.items():
@@ -72,6 +76,16 @@ def load_library(path=LIB_PATH):
 
 def _p(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def measure_fp64_peak(device=-1):
+    """GFLOP/s of an FP64 FMA-chain kernel on the current device."""
+    L = load_library()
+    g = C.c_double(0.0)
+    rc = L.imex_gpu_measure_fp64_peak(int(device), C.byref(g))
+    if rc != IMEX_OK:
+        raise ImexError(rc, "imex_gpu_measure_fp64_peak")
+    return g.value
 
 
 class ImexSolver:
@@ -107,11 +121,20 @@ class ImexSolver:
 
     # -- state
     def set_state(self, q, t=0.0):
-        q = np.ascontiguousarray(np.asarray(q, dtype=np.float64).ravel(order="F"))
+        """q: (n_vars,nx,ny) array, or a flat float64 array already in Fortran
+        element order (used as is, e.g. a pinned host buffer)."""
+        if not (isinstance(q, np.ndarray) and q.ndim == 1 and q.dtype == np.float64
+                and q.flags.c_contiguous):
+            q = np.ascontiguousarray(np.asarray(q, dtype=np.float64).ravel(order="F"))
         return self._check(self.lib.imex_gpu_set_state(self._h, _p(q), float(t)), "set_state")
 
-    def get_state(self, with_qp=False):
+    def get_state(self, with_qp=False, out=None):
+        """Returns q (n_vars,nx,ny); with `out` (flat float64, n_vars*nx*ny
+        elements) the state is written there and `out` is returned."""
         n = self.nx * self.ny
+        if out is not None and not with_qp:
+            self._check(self.lib.imex_gpu_get_state(self._h, _p(out), None), "get_state")
+            return out
         q = np.zeros(self.nv * n)
         qp = np.zeros((self.nv + 2) * n) if with_qp else None
         self._check(self.lib.imex_gpu_get_state(self._h, _p(q), _p(qp) if with_qp else None),
@@ -182,6 +205,24 @@ class ImexSolver:
 
     def sync(self):
         return self._check(self.lib.imex_gpu_sync(self._h), "sync")
+
+    def set_stream(self, stream_handle):
+        """Run on a caller's cudaStream_t (an int handle, e.g.
+        torch.cuda.current_stream().cuda_stream); 0/None = own stream."""
+        return self._check(self.lib.imex_gpu_set_stream(self._h, C.c_void_p(stream_handle or None)),
+                           "set_stream")
+
+    KERNELS = ("mask", "flux", "stage2")
+
+    def profile(self, enable=True):
+        return self._check(self.lib.imex_gpu_profile(self._h, int(bool(enable))), "profile")
+
+    def kernel_times(self):
+        """{kernel: (total_ms, launches)} since the last call (profile on)."""
+        ms = (C.c_double * 3)()
+        n = (C.c_int64 * 3)()
+        self._check(self.lib.imex_gpu_kernel_times(self._h, ms, n, 3), "kernel_times")
+        return {k: (ms[i], n[i]) for i, k in enumerate(self.KERNELS)}
 
     def device_state(self):
         p = C.POINTER(C.c_double)()

@@ -209,10 +209,26 @@ const char* imex_gpu_last_error(ImexCtx* ctx);
 /* Synchronise the context stream (for host timing of asynchronous work). */
 int imex_gpu_sync(ImexCtx* ctx);
 
+/* Run the context's work on a caller's CUDA stream (a cudaStream_t; NULL
+ * returns to the context's own stream), e.g. a framework's current stream so
+ * that its events time the step. */
+int imex_gpu_set_stream(ImexCtx* ctx, void* stream);
+
 /* Device-resident buffers for callers that bring their own device arrays
  * (benchmarks): SoA planes q[v][k][pitch] of the context, and its pitch in
  * elements.  The pointer stays valid for the context's life. */
 int imex_gpu_device_state(ImexCtx* ctx, double** q_dev, int64_t* pitch);
+
+/* Measurement helpers (no counterpart in the reference).
+ * imex_gpu_profile(ctx, 1) records CUDA events around the mask, flux and
+ * stage-2 kernels that imex_gpu_advance launches without a graph, on the
+ * context stream; imex_gpu_kernel_times returns, per kernel id (0 mask,
+ * 1 flux, 2 stage 2), the summed event time in ms and the launch count since
+ * the last call.  imex_gpu_measure_fp64_peak times an FP64 FMA-chain kernel
+ * and returns the achieved GFLOP/s (2 flops per FMA). */
+int imex_gpu_profile(ImexCtx* ctx, int enable);
+int imex_gpu_kernel_times(ImexCtx* ctx, double* total_ms, int64_t* launches, int n_kernels);
+int imex_gpu_measure_fp64_peak(int device, double* gflops);
 
 /* Build information: "sm_100a fmad=0 ..." */
 const char* imex_gpu_build_info(void);

@@ -1,0 +1,139 @@
+"""Small run set-ups shared by the parity tests (seeded, synthetic)."""
+import numpy as np
+
+from imex_sflow2d_v2_b200 import configs
+
+
+def dambreak(rheology=None, n=40, **kw):
+    return configs.dambreak(nx=n, ny=n, dx=0.25, rheology=rheology, **kw)
+
+
+def dambreak_variants():
+    out = {}
+    out["dambreak"] = dambreak()
+    out["dambreak_voellmy"] = dambreak(rheology=1)
+    out["dambreak_quadratic"] = dambreak(rheology=6)
+    p, st, q = dambreak(rheology=1)
+    p.alpha_flag = 1
+    qp = np.zeros((7, p.nx, p.ny))
+    _, xc, _, _ = configs.grid(p)
+    h = np.where(np.repeat(xc[:, None], p.ny, axis=1) < 5.0, 1.0, 0.1)
+    qp[0] = h
+    qp[3] = 300.0
+    qp[4] = 0.01
+    out["dambreak_alpha_flag"] = (p, st, configs.qp_to_qc_grid(p, qp))
+    p, st, q = dambreak(rheology=1)
+    p.energy_flag = 0
+    qp = np.zeros((7, p.nx, p.ny))
+    qp[0] = h
+    qp[3] = 300.0
+    qp[4] = 0.01 * h
+    out["dambreak_no_energy"] = (p, st, configs.qp_to_qc_grid(p, qp))
+    for lim in (2, 3, 4):
+        p, st, q = dambreak(rheology=1)
+        for i in range(7):
+            p.limiter[i] = lim
+        p.theta = 1.3
+        out["dambreak_limiter%d" % lim] = (p, st, q)
+    p, st, q = dambreak(rheology=1)
+    for side in "WESN":  # closed walls: reflective Dirichlet on hu/hv
+        configs.set_bc(p, side, 1, 0, 0.0)
+        configs.set_bc(p, side, 2, 0, 0.0)
+    out["dambreak_dirichlet"] = (p, st, q)
+    return out
+
+
+def sloped(n=48, dx=4.0, rheology=1, slope=True, curvature=True, seed=7):
+    """Wet slab on a seeded rough incline with the slope and curvature
+    corrections switched on."""
+    p = configs.default_params(n, n, 2, dx)
+    for i in range(2):
+        p.rho_s[i] = 2500.0
+        p.diam_s[i] = (1e-4, 1e-3)[i]
+        p.sp_heat_s[i] = 1617.0
+    p.rheology_flag = 1
+    p.rheology_model = rheology
+    p.mu, p.xi, p.friction_factor = 0.1, 500.0, 1e-3
+    p.max_dt = 1.0
+    configs.transmissive_bcs(p)
+    B = configs.fractal_dem(n, dx, 0.8, 30.0, 10.0, seed)
+    st = {"B_cent": B, "solve_mask_time": np.zeros((n, n))}
+    geom = configs.topography_geom(B, dx, dx)
+    st.update(geom)
+    if slope:
+        p.slope_correction_flag = 1
+        gc = 1.0 / (1.0 + geom["B_prime_x_geom"] ** 2 + geom["B_prime_y_geom"] ** 2)
+        st["grav_coeff"] = gc
+        st["d_grav_coeff_dx"] = -2.0 * gc ** 2 * (geom["B_prime_x_geom"] * geom["B_second_xx_geom"]
+                                                  + geom["B_prime_y_geom"] * geom["B_second_xy_geom"])
+        gsx = np.ones((n + 1, n))
+        gsx[1:n] = 0.5 * (gc[:-1] + gc[1:])
+        gsx[0] = gc[0]
+        gsx[n] = gc[-1]
+        gsy = np.ones((n, n + 1))
+        gsy[:, 1:n] = 0.5 * (gc[:, :-1] + gc[:, 1:])
+        gsy[:, 0] = gc[:, 0]
+        gsy[:, n] = gc[:, -1]
+        st["grav_coeff_stag_x"] = gsx
+        st["grav_coeff_stag_y"] = gsy
+    if curvature:
+        p.curvature_term_flag = 1
+    rng = np.random.default_rng(seed)
+    qp = np.zeros((8, n, n))
+    _, xc, _, yc = configs.grid(p)
+    X, Y = np.meshgrid(xc, yc, indexing="ij")
+    blob = np.exp(-((X - 0.3 * n * dx) ** 2 + (Y - 0.5 * n * dx) ** 2) / (2 * (0.15 * n * dx) ** 2))
+    h = 2.0 * blob * (blob > 0.05)
+    qp[0] = h
+    qp[1] = h * 1.0
+    qp[3] = 600.0 + 50.0 * rng.random((n, n))
+    qp[4] = 0.01 * h
+    qp[5] = 0.005 * h
+    qp[6] = np.where(h > 0, 1.0, 0.0)
+    return p, st, configs.qp_to_qc_grid(p, qp)
+
+
+def radial(n=64):
+    return configs.radial_current(nx=n, ny=n, dx=2.0, r_source=8.0, bump_sigma=30.0, mfr=5e5)
+
+
+def fractal_small(n=64, layer=1.0, seed=20261203):
+    """Third workload's physics (3 classes, settling + erosion, inlet) on a
+    small fractal DEM with an initial layer."""
+    return configs.fractal_inlet(n=n, dx=10.0, relief=120.0, seed=seed, r_source=25.0,
+                                 mfr=2e5, initial_layer=layer)
+
+
+def test2d():
+    """The reference's TESTS/TEST_2D run (100x68, quadratic friction, settling
+    and entrainment) from the committed input fixture."""
+    import os
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "test2d_inputs.npz"))
+    nx, ny = int(d["nx"]), int(d["ny"])
+    p = configs.default_params(nx, ny, 1, float(d["cell_size"]), x0=float(d["x0"]),
+                               y0=float(d["y0"]))
+    p.rho_s[0] = 2000.0
+    p.diam_s[0] = 1e-4
+    p.sp_heat_s[0] = 1617.0
+    p.settling_flag = 1
+    p.entrainment_flag = 1
+    p.erosion_coeff = 0.0
+    p.erodible_porosity = 0.0
+    p.erodible_fract[0] = 1.0
+    p.T_erodible = 300.0
+    p.rho_c_sub = p.pres / (p.sp_gas_const_a * p.T_erodible)
+    p.coeff_porosity = 0.0
+    p.rheology_flag = 1
+    p.rheology_model = 6
+    p.friction_factor = 1.0e-3
+    p.max_dt = 1.0
+    p.theta = 1.3
+    for side in "WESN":
+        for i in range(5):
+            configs.set_bc(p, side, i, 1, 0.0)
+    B = np.asfortranarray(d["B_cent"])
+    st = {"B_cent": B, "solve_mask_time": np.zeros((nx, ny)),
+          "erodible": np.zeros((1, nx, ny)), "deposit": np.zeros((nx, ny, 1)),
+          "erosion": np.zeros((nx, ny, 1))}
+    st.update(configs.topography_geom(B, p.cell_size, p.cell_size))
+    return p, st, np.asfortranarray(d["q"])
