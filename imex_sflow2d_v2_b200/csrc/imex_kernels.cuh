@@ -724,8 +724,10 @@ __device__ NewtonOut<NS> solve_rk_step(const DevParams& P, double* qj, const dou
       } else {
         double alam = 1.0;
         // every backtrack after the first halves alam: the cubic model's
-        // value is clamped to <= alam/2 and then maxed with alam/2
-        for (int trial = 0; trial < 4096; ++trial) {
+        // value is clamped to <= alam/2 and then maxed with alam/2.  The
+        // trials are capped at 4096; the cap exits like alam < alamin.
+        int trial;
+        for (trial = 0; trial < 4096; ++trial) {
           double qt[NV];
 #pragma unroll
           for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i] + alam * dd[i];
@@ -746,6 +748,11 @@ __device__ NewtonOut<NS> solve_rk_step(const DevParams& P, double* qj, const dou
           } else {
             alam = 0.5 * alam;
           }
+        }
+        if (trial == 4096) {
+#pragma unroll
+          for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i];
+          scal_f = scal_f_old;
         }
       }
     } else {
@@ -828,7 +835,7 @@ __device__ __noinline__ void mass_exchange(const DevParams& P, const double* qpj
     if (al[i] > 0.0 && P.settling_flag) {
       double sv = settling_velocity(P, P.diam_s[i], P.rho_s[i], m.rho_c, ikv);
       dep[i] = al[i] * sv * 1.0;
-      dep[i] = dep[i] * pow(1.0 - fmin_f(1.0, at / alpha_max), hind_exp);
+      dep[i] = dep[i] * ipow(1.0 - fmin_f(1.0, at / alpha_max), hind_exp);
       dep[i] = fmin_f(dep[i], r_h * al[i] / dtl);
       if (dep[i] < 0.0) dep_neg = true;
     }
@@ -846,7 +853,7 @@ __device__ __noinline__ void mass_exchange(const DevParams& P, const double* qpj
   double T_erod = P.erodible_deposit_flag ? r_T : P.T_erodible;
   double air_entr = 0.0;
   if (P.entrainment_flag && r_h > 0.0 && m.Ri > 0.0) {
-    double entr_coeff = 0.075 / sqrt(1.0 + 718.0 * pow(m.Ri, 2.4));
+    double entr_coeff = 0.075 / sqrt(1.0 + 718.0 * ipow(m.Ri, 2.4));
     air_entr = entr_coeff * sqrt(mv2);
   }
   double dep_tot = 0.0, ers_tot = 0.0, rdt = 0.0, ret = 0.0;

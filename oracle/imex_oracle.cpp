@@ -44,6 +44,7 @@ constexpr double EPS = 2.220446049250313e-16;  // EPSILON(1.0_wp)
 constexpr int MAXV = IMEX_MAX_VARS;
 constexpr int MAXP = IMEX_MAX_VARS + 2;
 constexpr int MAXS = IMEX_MAX_SOLID;
+constexpr int LNSRCH_MAX_TRIALS = 4096;
 
 // MIN/MAX with a defined answer for NaN operands (the non-NaN one).
 inline double fmin_f(double a, double b) {
@@ -55,6 +56,82 @@ inline double fmax_f(double a, double b) {
   if (std::isnan(a)) return b;
   if (std::isnan(b)) return a;
   return (b > a) ? b : a;
+}
+
+// x**y for the non-integer exponents of the mass-exchange closures
+// (settling drag, hindered settling, entrainment, inlet ramps).  Both the CPU
+// oracle and the CUDA path evaluate it with this same sequence of IEEE
+// operations, so the two agree bit for bit; the sequence is
+//   log x = e*ln2 + 2*atanh(s), s = (m-1)/(m+1), m in [sqrt(1/2), sqrt(2)),
+//           atanh by its odd Taylor series to s^23,
+//   z = y*log x carried as an unevaluated sum of two doubles (Dekker's exact
+//       product with Veltkamp splitting, Knuth's two-sum),
+//   exp z = 2^k * exp(r), r = z - k*ln2 (ln2 split in two), exp(r) by its
+//           Taylor series to r^17.
+// Accuracy against the exact power: within 4 ulp (measured); the reference's
+// libm pow is within 1 ulp, so results differ from it at that level only.
+inline void two_sum(double a, double b, double& s, double& e) {
+  s = a + b;
+  double bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
+}
+inline void two_prod(double a, double b, double& p, double& e) {
+  p = a * b;
+  double c = 134217729.0 * a;
+  double ah = c - (c - a), al = a - ah;
+  c = 134217729.0 * b;
+  double bh = c - (c - b), bl = b - bh;
+  e = ((ah * bh - p) + ah * bl + al * bh) + al * bl;
+}
+double ipow(double x, double y) {
+  if (std::isnan(x) || std::isnan(y)) return x + y;
+  if (x == 0.0 && y != 0.0) return (y > 0.0) ? 0.0 : HUGE_VAL;
+  if (x < 0.0 && y != 0.0) return std::nan("");
+  if (std::isinf(x) && y != 0.0) return (y > 0.0) ? x : 0.0;
+  if (y == 0.0) return 1.0;
+  if (x == 1.0) return 1.0;
+  const double LN2_HI = 0x1.62e42fee00000p-1, LN2_LO = 0x1.a39ef35793c76p-33;
+  const double INV_LN2 = 0x1.71547652b82fep+0, SQRTH = 0x1.6a09e667f3bcdp-1;
+  int e;
+  double m = std::frexp(x, &e);
+  if (m < SQRTH) {
+    m = m * 2.0;
+    e = e - 1;
+  }
+  double f = m - 1.0;
+  double s = f / (2.0 + f);
+  double s2 = s * s;
+  static const double inv_odd[11] = {0x1.5555555555555p-2, 0x1.999999999999ap-3, 0x1.2492492492492p-3,
+                                     0x1.c71c71c71c71cp-4, 0x1.745d1745d1746p-4, 0x1.3b13b13b13b14p-4,
+                                     0x1.1111111111111p-4, 0x1.e1e1e1e1e1e1ep-5, 0x1.af286bca1af28p-5,
+                                     0x1.8618618618618p-5, 0x1.642c8590b2164p-5};
+  double P = inv_odd[10];
+  for (int k = 9; k >= 0; --k) P = inv_odd[k] + s2 * P;
+  double ts = 2.0 * s;
+  double logm = ts + ts * (s2 * P);
+  double hi, lo;
+  two_sum((double)e * LN2_HI, logm, hi, lo);
+  lo = lo + (double)e * LN2_LO;
+  double p, pe;
+  two_prod(y, hi, p, pe);
+  pe = pe + y * lo;
+  double zh, zl;
+  two_sum(p, pe, zh, zl);
+  if (zh > 709.78) return HUGE_VAL;
+  if (zh < -745.1) return 0.0;
+  double kf = std::nearbyint(zh * INV_LN2);
+  double rh, rl;
+  two_sum(zh, -(kf * LN2_HI), rh, rl);
+  double r = rh + (rl + (zl - kf * LN2_LO));
+  static const double fact[18] = {0x1.0000000000000p+0, 0x1.0000000000000p+0, 0x1.0000000000000p-1,
+                                  0x1.5555555555555p-3, 0x1.5555555555555p-5, 0x1.1111111111111p-7,
+                                  0x1.6c16c16c16c17p-10, 0x1.a01a01a01a01ap-13, 0x1.a01a01a01a01ap-16,
+                                  0x1.71de3a556c734p-19, 0x1.27e4fb7789f5cp-22, 0x1.ae64567f544e4p-26,
+                                  0x1.1eed8eff8d898p-29, 0x1.6124613a86d09p-33, 0x1.93974a8c07c9dp-37,
+                                  0x1.ae7f3e733b81fp-41, 0x1.ae7f3e733b81fp-45, 0x1.952c77030ad4ap-49};
+  double E = fact[17];
+  for (int k = 16; k >= 0; --k) E = fact[k] + r * E;
+  return std::ldexp(E, (int)kf);
 }
 
 // ---------------------------------------------------------------- complex
@@ -680,7 +757,7 @@ double OracleCtx::settling_velocity(double diam, double rhos, double rhoc,
   if (Rey <= 1000.0) {
     for (int i = 1; i <= 20; ++i) {
       double sv_old = sv;
-      inv_sqrt_C_D = std::sqrt(Rey / (24.0 * (1.0 + 0.15 * std::pow(Rey, 0.687))));
+      inv_sqrt_C_D = std::sqrt(Rey / (24.0 * (1.0 + 0.15 * ipow(Rey, 0.687))));
       sv = const_part * inv_sqrt_C_D;
       if (std::fabs(sv_old - sv) / sv_old < 1.0e-6) return sv;
       Rey = diam * sv * ikv;
@@ -738,7 +815,7 @@ void OracleCtx::eval_mass_exchange_terms(const double* qpj, double bx, double by
     if (r_alphas[i] > 0.0 && p.settling_flag) {
       double sv = settling_velocity(p.diam_s[i], p.rho_s[i], rhoc, inv_kin_visc);
       dep[i] = r_alphas[i] * sv * 1.0;
-      dep[i] = dep[i] * std::pow(1.0 - fmin_f(1.0, alphas_tot / alpha_max), hind_exp);
+      dep[i] = dep[i] * ipow(1.0 - fmin_f(1.0, alphas_tot / alpha_max), hind_exp);
       dep[i] = fmin_f(dep[i], r_h * r_alphas[i] / dtl);
       if (dep[i] < 0.0) err |= IMEX_ERRBIT(IMEX_EEROSION);
     }
@@ -754,7 +831,7 @@ void OracleCtx::eval_mass_exchange_terms(const double* qpj, double bx, double by
   double T_erodible = p.erodible_deposit_flag ? r_T : p.T_erodible;
   double air_entr;
   if (p.entrainment_flag && r_h > 0.0 && r_Ri > 0.0) {
-    double entr_coeff = 0.075 / std::sqrt(1.0 + 718.0 * std::pow(r_Ri, 2.4));
+    double entr_coeff = 0.075 / std::sqrt(1.0 + 718.0 * ipow(r_Ri, 2.4));
     air_entr = entr_coeff * std::sqrt(mod_vel2);
   } else {
     air_entr = 0.0;
@@ -811,7 +888,7 @@ void OracleCtx::eval_source_bdry(double time, double vx, double vy, double* sb) 
     else if (t_rem <= tp[1])
       t_coeff = 0.5 * (1.0 + std::cos(pi_g * ((t_rem - tp[1]) / tp[2] + 1.0)));
   }
-  double tc15 = std::pow(t_coeff, 1.5), tc05 = std::pow(t_coeff, 0.5);
+  double tc15 = ipow(t_coeff, 1.5), tc05 = ipow(t_coeff, 0.5);
   sb[0] = t_coeff * p.h_source;
   sb[1] = tc15 * p.h_source * p.vel_source * vx;
   sb[2] = tc15 * p.h_source * p.vel_source * vy;
@@ -1512,7 +1589,16 @@ void OracleCtx::lnsrch(const double* x_old, const double* qj_org, const double* 
   }
   double alam = 1.0, alam2 = 0.0, scal_f2 = 0.0, tmplam = 0.0;
   double qj[MAXV];
-  for (;;) {
+  // the reference loop ends only through the two exits below; a non-finite
+  // first backtrack would keep alam from shrinking, so the trials are capped
+  // (the CUDA path uses the same cap) and the cap exits like alam < alamin
+  for (int ntrial = 0;; ++ntrial) {
+    if (ntrial == LNSRCH_MAX_TRIALS) {
+      for (int i = 0; i < nv; ++i) qj_rel[i] = x_old[i];
+      scal_f = scal_f_old;
+      check = true;
+      break;
+    }
     for (int i = 0; i < nv; ++i) qj_rel[i] = x_old[i] + alam * desc_dir[i];
     for (int i = 0; i < nv; ++i) qj[i] = qj_rel[i] * qj_org[i];
     eval_f(qj, qj_old, a_diag, coeff_f, Rj_not_impl, bx, by, dtl, right_term, scal_f);
@@ -2300,6 +2386,8 @@ int oracle_solve_rk_step(OracleCtx* o, double* qj, const double* qj_old,
   int64_t trials = 0;
   return o->solve_rk_step(qj, qj_old, a_diag, rj_not_impl, bprime_x, bprime_y, dt, trials);
 }
+
+double oracle_ipow(double x, double y) { return ipow(x, y); }
 
 double oracle_limit(double v1, double v2, double v3, double z1, double z2, double z3,
                     int limiter, double theta) {

@@ -63,6 +63,7 @@ void oracle_implicit_terms(OracleCtx* o, const double* q_re, const double* q_im,
 int oracle_solve_rk_step(OracleCtx* o, double* qj, const double* qj_old,
                          const double* rj_not_impl, double bprime_x,
                          double bprime_y, double dt, double a_diag);
+double oracle_ipow(double x, double y);
 double oracle_limit(double v1, double v2, double v3, double z1, double z2,
                     double z3, int limiter, double theta);
 

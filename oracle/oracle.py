@@ -63,6 +63,8 @@ def lib():
         L.oracle_solve_rk_step.restype = C.c_int
         L.oracle_solve_rk_step.argtypes = [vp, dp, dp, dp, C.c_double, C.c_double,
                                            C.c_double, C.c_double]
+        L.oracle_ipow.restype = C.c_double
+        L.oracle_ipow.argtypes = [C.c_double, C.c_double]
         L.oracle_limit.restype = C.c_double
         L.oracle_limit.argtypes = [C.c_double] * 6 + [C.c_int, C.c_double]
         _LIB = L
@@ -188,6 +190,10 @@ class Oracle:
         it = lib().oracle_solve_rk_step(self._h, _p(qj), _p(qo), _p(rj), float(bx), float(by),
                                         float(dt), float(a_diag))
         return qj, it
+
+
+def ipow(x, y):
+    return lib().oracle_ipow(float(x), float(y))
 
 
 def limit(v1, v2, v3, z1, z2, z3, limiter, theta=1.0):

@@ -1,10 +1,9 @@
 """Parity of the sm_100a path with the CPU oracle, through the C ABI.
 
-Bit-exact where the arithmetic is +,-,*,/,sqrt (the dam-break, inlet and
-slope cases): solve masks, CFL dt and every conserved variable equal bit for
-bit after every step.  Cases that evaluate pow() (settling velocity, hindered
-settling, entrainment) compare within relative L1 <= 1e-10, the tolerance the
-rebuild is held to; their masks must still match exactly."""
+Solve masks, CFL dt, every conserved variable and the erosion/deposition
+planes equal bit for bit after every step, in every case (the power laws of
+the mass-exchange closures use the same explicitly written x**y on both
+sides).  The north-star tolerance, relative L1 <= 1e-10, is asserted too."""
 import numpy as np
 import pytest
 
@@ -55,16 +54,14 @@ def test_slope_and_curvature_bitexact(rheology):
     assert_bitexact(recs, allow_errors=True)
 
 
-def test_reference_test2d_within_tolerance():
+def test_reference_test2d_bitexact():
     p, st, q = cases.test2d()
-    recs, o, g = lockstep(p, st, q, 60, erosion=True)
+    recs, o, g = lockstep(p, st, q, 80, erosion=True)
+    assert_bitexact(recs)
     for r in recs:
-        assert r["mask_equal"], r
-        assert r["rel_l1"] <= 1e-10, r
-        assert r["dt"][1] == pytest.approx(r["dt"][0], rel=1e-10)
-    er_o, de_o, eo_o, _ = o.get_exchange()
-    er_g, de_g, eo_g, _ = g.get_exchange()
-    assert rel_l1(de_o, de_g) <= 1e-10
+        assert r["rel_l1"] <= 1e-10
+    for a, b in zip(o.get_exchange(), g.get_exchange()):
+        np.testing.assert_array_equal(a, b)
 
 
 def test_fractal_erosion_through_advance():
@@ -80,14 +77,12 @@ def test_fractal_erosion_through_advance():
     for step in range(40):
         eo, to = o.advance(1)
         eg, tg = g.advance(1)
-        assert tg == pytest.approx(to, rel=1e-12)
+        assert tg == to, step
         qo, qg = o.get_state(), g.get_state()
-        assert rel_l1(qo, qg) <= 1e-10, step
-    er_o, de_o, eo_o, _ = o.get_exchange()
-    er_g, de_g, eo_g, _ = g.get_exchange()
-    assert rel_l1(er_o, er_g) <= 1e-10
-    assert rel_l1(de_o, de_g) <= 1e-10
-    assert rel_l1(eo_o, eo_g) <= 1e-10
+        np.testing.assert_array_equal(qo, qg)
+        assert np.array_equal(o.get_masks()[0], g.get_masks()[0]), step
+    for a, b in zip(o.get_exchange(), g.get_exchange()):
+        np.testing.assert_array_equal(a, b)
 
 
 def test_advance_graph_equals_stepwise():

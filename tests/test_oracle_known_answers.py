@@ -5,7 +5,7 @@ import pytest
 
 import cases
 from imex_sflow2d_v2_b200 import configs
-from oracle import Oracle, limit
+from oracle import Oracle, ipow, limit
 
 
 def run_oracle(p, st, q, n, dt0=1e-3):
@@ -138,3 +138,17 @@ def test_test2d_fixture_runs_clean():
     s = o.stats()
     assert s.newton_cells > 0
     assert o.stale_wet_reads() == 0
+
+
+def test_ipow_accuracy_and_special_values():
+    from decimal import Decimal, getcontext
+    import math
+    getcontext().prec = 50
+    rng = np.random.default_rng(5)
+    for y in (0.687, 4.65, 2.4, 1.5, 0.5):
+        for x in np.concatenate([rng.uniform(0, 1, 300), rng.uniform(1, 1e3, 300),
+                                 10 ** rng.uniform(-10, 6, 300)]):
+            exact = float(Decimal(float(x)) ** Decimal(y))
+            assert abs(ipow(x, y) - exact) <= 4 * math.ulp(exact), (x, y)
+    assert ipow(1.0, 1.5) == 1.0 and ipow(0.0, 0.5) == 0.0 and ipow(2.0, 0.0) == 1.0
+    assert math.isnan(ipow(-1.0, 0.5)) and ipow(-1.0, 0.0) == 1.0
