@@ -875,3 +875,206 @@ int imex_gpu_device_state(ImexCtx* ctx, double** q_dev, int64_t* pitch) {
 }
 
 }  // extern "C"
+
+// ======================================================= allocation-free dt
+// imex_gpu_timestep_noalloc: the CFL time step of imex_gpu_timestep for
+// callers that may not allocate device memory when they call it, e.g. a
+// driver whose GPU memory is a fixed pool owned by another framework, where
+// a new allocation would fail or break the pool's accounting.  It allocates
+// nothing: its only scratch is the file-scope array below, one partial
+// minimum per 32x8 tile plus one result slot.  Every call writes all the
+// slots it later reads, so nothing needs to start at zero; calls that run at
+// the same time on one GPU share the array and race.
+namespace {
+constexpr int NOALLOC_MAX_TILES = 1 << 20;  // 8 MiB of doubles + 1 result slot
+}  // namespace
+static __device__ __align__(256) double g_noalloc_dt[NOALLOC_MAX_TILES + 1];
+
+namespace {
+// Device address of g_noalloc_dt, looked up once per device (host code may
+// not use the symbol's name as a device address).
+constexpr int NOALLOC_MAX_DEVICES = 64;
+double* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
+
+// Per-tile CFL minimum.  k_flux takes its speeds from the stage view and,
+// when an inlet-interior cell is in the stencil, from the timestep view;
+// the two views differ only at inlet-interior cells, so taking the timestep
+// view everywhere gives the same speeds.  The fluxes are discarded.
+template <int NS>
+__global__ void __launch_bounds__(FLUX_THREADS)
+    k_cfl_tiles(const DevParams* __restrict__ Pp, const double* __restrict__ q,
+                const uint8_t* __restrict__ mask, const uint8_t* __restrict__ cellinfo,
+                const double* __restrict__ gcsx, const double* __restrict__ gcsy,
+                const RingCell* __restrict__ ring, const DevClock* clk, double* tile_min) {
+  constexpr int NV = 4 + NS, NP = 6 + NS;
+  const DevParams& P = *Pp;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FluxShared<NS>& S = *reinterpret_cast<FluxShared<NS>*>(smem_raw);
+  const int j0 = blockIdx.x * TX, k0 = blockIdx.y * TY;
+  const int nx = P.nx, ny = P.ny;
+  const long long tile = (long long)blockIdx.y * gridDim.x + blockIdx.x;
+  const double time = clk->t;
+  int any = 0;
+  for (int e = threadIdx.x; e < TX * TY; e += blockDim.x) {
+    int j = j0 + e % TX, k = k0 + e / TX;
+    if (j < nx && k < ny && mask[(size_t)k * P.pitch + j]) any = 1;
+  }
+  if (!__syncthreads_or(any)) {
+    if (threadIdx.x == 0) tile_min[tile] = P.max_dt;
+    return;
+  }
+  for (int e = threadIdx.x; e < SW * SH; e += blockDim.x) {
+    int lx = e % SW, ly = e / SW;
+    int j = j0 + lx - HALO, k = k0 + ly - HALO;
+    double qc[NV], qpv[NP];
+    uint8_t inf = 0;
+    if (j >= 0 && j < nx && k >= 0 && k < ny) {
+      size_t c = (size_t)k * P.pitch + j;
+      inf = P.has_cellinfo ? cellinfo[(size_t)k * nx + j] : 0;
+      if (mask[c]) inf |= 128;
+      if (P.radial_source_flag && (inf & CI_SRC_MASK) == 1) {
+#pragma unroll
+        for (int i = 0; i < NP; ++i) qpv[i] = 0.0;
+        qpv[3] = P.T_ambient;
+      } else {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) qc[i] = q[c + (size_t)i * P.plane];
+        cell_qp<NS>(P, qc, qpv);
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < NP; ++i) qpv[i] = 0.0;
+    }
+#pragma unroll
+    for (int i = 0; i < NP; ++i) S.tile.qp[i][ly][lx] = qpv[i];
+    S.tile.info[ly][lx] = inf;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < NXI + NYI; e += blockDim.x) {
+    double H[NV], amax = 0.0, aN, aP;
+    if (e < NXI) {
+      int jj = e % (TX + 1), kk = e / (TX + 1);
+      int ja = j0 + jj - 1, ka = k0 + kk, ia_x = jj - 1 + HALO, ia_y = kk + HALO;
+      S.ax[kk][jj] = 0.0;
+      if (ka >= ny || ja + 1 > nx) continue;
+      bool a_in = ja >= 0, b_in = ja + 1 < nx;
+      bool sa = a_in && (S.tile.info[ia_y][ia_x] & 128);
+      bool sb = b_in && (S.tile.info[ia_y][ia_x + 1] & 128);
+      if (!(sa || sb)) continue;
+      double gcf = P.slope_correction_flag ? gcsx[(size_t)ka * (nx + 1) + (ja + 1)] : 1.0;
+      interface_flux<NS>(P, S.tile, 1, ia_x, ia_y, ja, ka, a_in, b_in, gcf, false, time, ring, H,
+                         amax, aN, aP);
+      S.ax[kk][jj] = amax;
+    } else {
+      int e2 = e - NXI;
+      int jj = e2 % TX, kk = e2 / TX;
+      int ja = j0 + jj, ka = k0 + kk - 1, ia_x = jj + HALO, ia_y = kk - 1 + HALO;
+      S.ay[kk][jj] = 0.0;
+      if (ja >= nx || ka + 1 > ny) continue;
+      bool a_in = ka >= 0, b_in = ka + 1 < ny;
+      bool sa = a_in && (S.tile.info[ia_y][ia_x] & 128);
+      bool sb = b_in && (S.tile.info[ia_y + 1][ia_x] & 128);
+      if (!(sa || sb)) continue;
+      double gcf = P.slope_correction_flag ? gcsy[(size_t)(ka + 1) * nx + ja] : 1.0;
+      interface_flux<NS>(P, S.tile, 2, ia_x, ia_y, ja, ka, a_in, b_in, gcf, false, time, ring, H,
+                         amax, aN, aP);
+      S.ay[kk][jj] = amax;
+    }
+  }
+  __syncthreads();
+  double dtl = P.max_dt;
+  for (int e = threadIdx.x; e < TX * TY; e += blockDim.x) {
+    int jj = e % TX, kk = e / TX;
+    int j = j0 + jj, k = k0 + kk;
+    if (j >= nx || k >= ny) continue;
+    if (!(S.tile.info[kk + HALO][jj + HALO] & 128)) continue;
+    double max_a = fmax_f(S.ax[kk][jj], S.ax[kk][jj + 1]);
+    double dtx = (max_a > 0.0) ? P.cfl * P.dx / max_a : dtl;
+    max_a = fmax_f(S.ay[kk][jj], S.ay[kk + 1][jj]);
+    double dty = (max_a > 0.0) ? P.cfl * P.dy / max_a : dtl;
+    dtl = fmin_f(dtl, fmin_f(dtx, dty));
+  }
+  for (int off = 16; off > 0; off >>= 1) dtl = fmin_f(dtl, __shfl_down_sync(0xffffffffu, dtl, off));
+  if ((threadIdx.x & 31) == 0) S.dtmin[threadIdx.x >> 5] = dtl;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = S.dtmin[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmin_f(m, S.dtmin[w]);
+    tile_min[tile] = m;
+  }
+}
+
+// One block folds the tile minima into slot n_tiles of the same array with
+// the rule of the atomic minimum in k_flux (only 0 < m < max_dt lowers dt).
+__global__ void __launch_bounds__(1024) k_cfl_fold(const DevParams* __restrict__ Pp,
+                                                   double* tile_min, long long n_tiles) {
+  __shared__ double red[32];
+  const double max_dt = Pp->max_dt;
+  double m = max_dt;
+  for (long long i = threadIdx.x; i < n_tiles; i += blockDim.x) {
+    double v = tile_min[i];
+    if (v > 0.0 && v < max_dt) m = fmin_f(m, v);
+  }
+  for (int off = 16; off > 0; off >>= 1) m = fmin_f(m, __shfl_down_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = red[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) r = fmin_f(r, red[w]);
+    tile_min[n_tiles] = r;
+  }
+}
+
+template <int NS>
+cudaError_t launch_cfl_tiles(ImexCtx* ctx, double* scratch) {
+  const DevParams& P = ctx->P;
+  size_t smem = sizeof(FluxShared<NS>);
+  cudaError_t e = cudaFuncSetAttribute(k_cfl_tiles<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  k_cfl_tiles<NS><<<tile_grid(P), FLUX_THREADS, smem, ctx->stream>>>(
+      ctx->dP, ctx->q, ctx->mask, ctx->cellinfo, ctx->gcsx, ctx->gcsy, ctx->ring, ctx->clk,
+      scratch);
+  ctx->launches += 1;
+  return cudaGetLastError();
+}
+}  // namespace
+
+extern "C" int imex_gpu_timestep_noalloc(ImexCtx* ctx, double* dt) {
+  if (!ctx || !dt) return IMEX_EINVAL;
+  CK(cudaSetDevice(ctx->device));
+  const dim3 g = tile_grid(ctx->P);
+  const long long n_tiles = (long long)g.x * g.y;
+  if (n_tiles > NOALLOC_MAX_TILES)
+    return fail(ctx, IMEX_EINVAL,
+                "imex_gpu_timestep_noalloc: grid needs " + std::to_string(n_tiles) +
+                    " tiles of 32x8 cells; the built-in scratch holds at most " +
+                    std::to_string(NOALLOC_MAX_TILES));
+  if (ctx->device < 0 || ctx->device >= NOALLOC_MAX_DEVICES)
+    return fail(ctx, IMEX_EINVAL, "imex_gpu_timestep_noalloc: device index out of range");
+  if (!g_noalloc_ptr[ctx->device]) {
+    // first call on this device: resolve the scratch array's device address
+    void* ptr = nullptr;
+    CK(cudaGetSymbolAddress(&ptr, g_noalloc_dt));
+    g_noalloc_ptr[ctx->device] = static_cast<double*>(ptr);
+  }
+  double* scratch = g_noalloc_ptr[ctx->device];
+  if (ctx->P.cfl == -1.0) {
+    *dt = ctx->P.max_dt;
+    return IMEX_OK;
+  }
+  cudaError_t e;
+  switch (ctx->ns) {
+    case 1: e = launch_cfl_tiles<1>(ctx, scratch); break;
+    case 2: e = launch_cfl_tiles<2>(ctx, scratch); break;
+    case 3: e = launch_cfl_tiles<3>(ctx, scratch); break;
+    default: e = launch_cfl_tiles<4>(ctx, scratch); break;
+  }
+  CK(e);
+  k_cfl_fold<<<1, 1024, 0, ctx->stream>>>(ctx->dP, scratch, n_tiles);
+  ctx->launches += 1;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(dt, scratch + n_tiles, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return IMEX_OK;
+}

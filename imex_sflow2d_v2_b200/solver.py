@@ -51,6 +51,7 @@ def load_library(path=LIB_PATH):
         "imex_gpu_get_exchange": ([vp, dp, dp, dp, dp], C.c_int),
         "imex_gpu_check_solve": ([vp, C.c_double, C.c_int, i64p], C.c_int),
         "imex_gpu_timestep": ([vp, dp], C.c_int),
+        "imex_gpu_timestep_noalloc": ([vp, dp], C.c_int),
         "imex_gpu_rk_step": ([vp, C.c_double, C.c_double], C.c_int),
         "imex_gpu_erosion_deposition": ([vp, C.c_double], C.c_int),
         "imex_gpu_get_masks": ([vp, i8p, i8p, i8p], C.c_int),
@@ -165,6 +166,13 @@ class ImexSolver:
     def timestep(self):
         dt = C.c_double(0.0)
         self._check(self.lib.imex_gpu_timestep(self._h, C.byref(dt)), "timestep")
+        return dt.value
+
+    def timestep_noalloc(self):
+        """CFL dt like timestep(), through the entry point that allocates
+        nothing (its scratch is a fixed array inside the library)."""
+        dt = C.c_double(0.0)
+        self._check(self.lib.imex_gpu_timestep_noalloc(self._h, C.byref(dt)), "timestep_noalloc")
         return dt.value
 
     def imex_RK_solver(self, t, dt):

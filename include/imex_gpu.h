@@ -184,6 +184,22 @@ int imex_gpu_get_exchange(ImexCtx* ctx, double* erodible, double* deposit,
 /* The reference's per-step routines, one call each. */
 int imex_gpu_check_solve(ImexCtx* ctx, double t, int solve_all, int64_t* n_solve_cells);
 int imex_gpu_timestep(ImexCtx* ctx, double* dt);
+
+/* The same CFL time step as imex_gpu_timestep, for callers that must not
+ * allocate device memory at the time of the call: drivers living under a
+ * fixed device-memory reservation (another framework's pool already owns the
+ * GPU) or running in phases where allocation calls are not allowed.  It has
+ * no counterpart in the reference.  Nothing is allocated: its only scratch
+ * is a fixed array built into the library (8 MiB, held on every GPU that
+ * loads it until exit), one slot per 32x8-cell tile, so grids above
+ * 1,048,576 tiles (about 268 million cells) are rejected with IMEX_EINVAL
+ * and a message in imex_gpu_last_error.  Inputs are the context's state and
+ * mask (from imex_gpu_check_solve); the output is *dt on the host.  Unlike
+ * imex_gpu_timestep it leaves the stage-1 fluxes uncomputed.  The first call
+ * on a device looks up the array's device address; make that first call
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on one GPU race with each other. */
+int imex_gpu_timestep_noalloc(ImexCtx* ctx, double* dt);
 int imex_gpu_rk_step(ImexCtx* ctx, double t, double dt);
 int imex_gpu_erosion_deposition(ImexCtx* ctx, double dt);
 

@@ -1,0 +1,51 @@
+"""imex_gpu_timestep_noalloc against imex_gpu_timestep on the same states.
+
+The allocation-free entry point must give the CFL dt of the ordinary one.
+Both are folds of the same per-interface speeds with an exact minimum, so the
+tolerance is zero: the two doubles are equal.  Each state is queried twice in
+a row through the new entry point, and a second, smaller grid follows a
+larger one so that tile minima left behind in the built-in scratch by the
+first grid cannot leak into the second."""
+import pytest
+
+import cases
+from imex_sflow2d_v2_b200.solver import ImexSolver
+
+pytestmark = pytest.mark.gpu
+
+DT_TOL = 0.0  # relative; exact minima of the same speeds
+
+
+def _close(a, b):
+    return abs(a - b) <= DT_TOL * max(abs(a), abs(b))
+
+
+def _walk(p, st, q, nsteps):
+    g = ImexSolver(p, st)
+    g.set_state(q, 0.0)
+    t = 0.0
+    seen = []
+    for _ in range(nsteps):
+        g.check_solve(t)
+        d1 = g.timestep_noalloc()
+        d2 = g.timestep_noalloc()
+        d0 = g.timestep()
+        assert _close(d1, d0), (d1, d0)
+        assert _close(d2, d0), (d2, d0)
+        seen.append(d0)
+        g.imex_RK_solver(t, d0)
+        t = t + d0
+    return seen
+
+
+def test_noalloc_dt_radial_then_dambreak():
+    p, st, q = cases.radial(n=64)
+    dts = _walk(p, st, q, 12)
+    assert all(0.0 < d <= p.max_dt for d in dts)
+    p, st, q = cases.dambreak(n=40)
+    _walk(p, st, q, 12)
+
+
+def test_noalloc_dt_fractal():
+    p, st, q = cases.fractal_small()
+    _walk(p, st, q, 6)
