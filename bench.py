@@ -67,9 +67,10 @@ def bytes_per_cell(ns, erosion):
     mask = 8 + 1                                   # q1 read, mask byte written
     flux = 8 * nv + 1 + 16 + 8 * nv                # q, mask, B'x, B'y read; X written
     stage2 = 8 * nv + 8 * nv + 1 + 16 + 8 * nv     # q, X, mask, B' read; q written
-    if erosion:
-        stage2 += 2 * 3 * 8 * ns                   # erodible, deposit, erosion read+write
-    return {"mask": mask, "flux": flux, "stage2": stage2}
+    out = {"mask": mask, "flux": flux, "stage2": stage2}
+    if erosion:                                    # q, mask, B' read; q written;
+        out["erosion"] = 8 * nv + 1 + 16 + 8 * nv + 2 * 3 * 8 * ns  # 3 planes per class r+w
+    return out
 
 
 class ClockSampler:

@@ -120,32 +120,23 @@ cudaError_t launch_flux(ImexCtx* ctx) {
   }
 }
 
-template <int NS, bool ER>
+template <int NS>
 cudaError_t launch_stage2_ns(ImexCtx* ctx) {
   const DevParams& P = ctx->P;
   int grid = grid_1d((long long)P.nx * P.ny, 128);
-  k_stage2<NS, ER><<<grid, 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->X, ctx->mask, ctx->cellinfo,
-                                                  ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy, ctx->Byy,
-                                                  ctx->gc, ctx->erodible, ctx->deposit,
-                                                  ctx->erosion, ctx->Bcent, ctx->clk);
+  k_stage2<NS><<<grid, 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->X, ctx->mask, ctx->cellinfo,
+                                              ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy, ctx->Byy,
+                                              ctx->gc, ctx->clk);
   ctx->launches += 1;
   return cudaGetLastError();
 }
 
-cudaError_t launch_stage2(ImexCtx* ctx, bool erosion) {
-  if (erosion) {
-    switch (ctx->ns) {
-      case 1: return launch_stage2_ns<1, true>(ctx);
-      case 2: return launch_stage2_ns<2, true>(ctx);
-      case 3: return launch_stage2_ns<3, true>(ctx);
-      default: return launch_stage2_ns<4, true>(ctx);
-    }
-  }
+cudaError_t launch_stage2(ImexCtx* ctx) {
   switch (ctx->ns) {
-    case 1: return launch_stage2_ns<1, false>(ctx);
-    case 2: return launch_stage2_ns<2, false>(ctx);
-    case 3: return launch_stage2_ns<3, false>(ctx);
-    default: return launch_stage2_ns<4, false>(ctx);
+    case 1: return launch_stage2_ns<1>(ctx);
+    case 2: return launch_stage2_ns<2>(ctx);
+    case 3: return launch_stage2_ns<3>(ctx);
+    default: return launch_stage2_ns<4>(ctx);
   }
 }
 
@@ -183,7 +174,7 @@ bool erosion_active(const ImexCtx* ctx) {
 }
 
 // Kernel ids for imex_gpu_kernel_times.
-enum { KID_MASK = 0, KID_FLUX = 1, KID_STAGE2 = 2, KID_N = 3 };
+enum { KID_MASK = 0, KID_FLUX = 1, KID_STAGE2 = 2, KID_EROSION = 3, KID_N = 4 };
 
 cudaEvent_t pool_event(ImexCtx* ctx) {
   if (ctx->ev_used == ctx->ev_pool.size()) {
@@ -214,7 +205,7 @@ struct ProfScope {
 };
 
 // Device part of one driver-loop pass: mask, fluxes + CFL, dt clip, stage 2
-// (+ erosion), t += dt.
+// , erosion/deposition, t += dt.
 cudaError_t enqueue_step(ImexCtx* ctx) {
   cudaError_t e;
   k_step_begin<<<1, 1, 0, ctx->stream>>>(ctx->clk, ctx->P.max_dt, 1);
@@ -231,7 +222,11 @@ cudaError_t enqueue_step(ImexCtx* ctx) {
   ctx->launches += 1;
   {
     ProfScope ps(ctx, KID_STAGE2);
-    if ((e = launch_stage2(ctx, erosion_active(ctx))) != cudaSuccess) return e;
+    if ((e = launch_stage2(ctx)) != cudaSuccess) return e;
+  }
+  if (erosion_active(ctx)) {
+    ProfScope ps(ctx, KID_EROSION);
+    if ((e = launch_erosion(ctx)) != cudaSuccess) return e;
   }
   k_step_end<<<1, 1, 0, ctx->stream>>>(ctx->clk);
   ctx->launches += 1;
@@ -653,7 +648,7 @@ int imex_gpu_rk_step(ImexCtx* ctx, double t, double dt) {
   int r = push_time(ctx, t, &dt);
   if (r) return r;
   if (!ctx->x_valid) CK(launch_flux(ctx));
-  CK(launch_stage2(ctx, false));
+  CK(launch_stage2(ctx));
   ctx->x_valid = false;
   return collect_errors(ctx);
 }

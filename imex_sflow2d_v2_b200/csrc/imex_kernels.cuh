@@ -8,9 +8,10 @@
 //               divergence, explicit terms and the CFL minimum
 //               (timestep + RK stage 1: src/solver_2d.f90:872-1005,2614-3918)
 //   k_stage2    RK stage 2 per cell: semi-implicit terms, Newton with line
-//               search and complex-step Jacobian, assembly checks, optionally
-//               the erosion/deposition update (src/solver_2d.f90:1105-1628,
-//               1660-2365, 2380-2595)
+//               search and complex-step Jacobian, assembly checks
+//               (src/solver_2d.f90:1105-1628, 1660-2365)
+//   k_erosion   the erosion/deposition update per cell
+//               (src/solver_2d.f90:2380-2595)
 //
 // Data layout: structure-of-arrays planes, plane v of q at q + v*plane,
 // element (j,k) (0-based) at k*pitch + j.
@@ -28,6 +29,18 @@ constexpr int SH = TY + 2 * HALO;  // shared tile height
 constexpr int FLUX_THREADS = 288;
 constexpr int NXI = (TX + 1) * TY;  // x-interfaces per tile
 constexpr int NYI = TX * (TY + 1);  // y-interfaces per tile
+
+// Minimum resident blocks per SM asked of ptxas for the flux and per-cell
+// kernels (their register budget); tuning knobs, set with -D at build time.
+#ifndef IMEX_STAGE2_MINB
+#define IMEX_STAGE2_MINB 8
+#endif
+#ifndef IMEX_EROSION_MINB
+#define IMEX_EROSION_MINB 8
+#endif
+#ifndef IMEX_FLUX_MINB
+#define IMEX_FLUX_MINB 2
+#endif
 
 // Device clock shared by the step kernels (graph-replayable).
 struct DevClock {
@@ -390,7 +403,7 @@ struct FluxShared {
 };
 
 template <int NS>
-__global__ void __launch_bounds__(FLUX_THREADS)
+__global__ void __launch_bounds__(FLUX_THREADS, IMEX_FLUX_MINB)
     k_flux(const DevParams* __restrict__ Pp, const double* __restrict__ q, const uint8_t* __restrict__ mask,
            const uint8_t* __restrict__ cellinfo, const double* __restrict__ Bx,
            const double* __restrict__ By, const double* __restrict__ Bxx,
@@ -948,15 +961,13 @@ __device__ bool erosion_cell(const DevParams& P, double* qc, double bx, double b
 }
 
 // =============================================================== k_stage2
-template <int NS, bool EROSION>
-__global__ void __launch_bounds__(128)
+template <int NS>
+__global__ void __launch_bounds__(128, IMEX_STAGE2_MINB)
     k_stage2(const DevParams* __restrict__ Pp, double* __restrict__ q, const double* __restrict__ X,
              const uint8_t* __restrict__ mask, const uint8_t* __restrict__ cellinfo,
              const double* __restrict__ Bx, const double* __restrict__ By,
              const double* __restrict__ Bxx, const double* __restrict__ Bxy,
-             const double* __restrict__ Byy, const double* __restrict__ gc,
-             double* __restrict__ erodible, double* __restrict__ deposit,
-             double* __restrict__ erosion, double* __restrict__ Bcent, DevClock* clk) {
+             const double* __restrict__ Byy, const double* __restrict__ gc, DevClock* clk) {
   const DevParams& P = *Pp;
   constexpr int NV = 4 + NS, NP = 6 + NS;
   const int nx = P.nx, ny = P.ny;
@@ -1094,26 +1105,6 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
       for (int i = 0; i < NV; ++i) qc[i] = 0.0;
     }
-    if (EROSION) {
-      double er[NS], de[NS], eo[NS], Bc = 0.0;
-      const size_t N = (size_t)P.plane;
-#pragma unroll
-      for (int i = 0; i < NS; ++i) {
-        er[i] = erodible[c + i * N];
-        de[i] = deposit[c + i * N];
-        eo[i] = erosion[c + i * N];
-      }
-      if (P.topo_change_flag) Bc = Bcent[c];
-      bool bad = erosion_cell<NS>(P, qc, bx, by, er, de, eo, &Bc, dt);
-#pragma unroll
-      for (int i = 0; i < NS; ++i) {
-        erodible[c + i * N] = er[i];
-        deposit[c + i * N] = de[i];
-        erosion[c + i * N] = eo[i];
-      }
-      if (P.topo_change_flag) Bcent[c] = Bc;
-      if (bad) record_error(clk, 6, cell);
-    }
 #pragma unroll
     for (int i = 0; i < NV; ++i) q[c + (size_t)i * P.plane] = qc[i];
   }
@@ -1134,7 +1125,7 @@ __global__ void __launch_bounds__(128)
 
 // Stand-alone erosion/deposition pass (imex_gpu_erosion_deposition).
 template <int NS>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, IMEX_EROSION_MINB)
     k_erosion(const DevParams* __restrict__ Pp, double* __restrict__ q, const uint8_t* __restrict__ mask,
               const double* __restrict__ Bx, const double* __restrict__ By,
               double* __restrict__ erodible, double* __restrict__ deposit,

@@ -220,16 +220,17 @@ class ImexSolver:
         return self._check(self.lib.imex_gpu_set_stream(self._h, C.c_void_p(stream_handle or None)),
                            "set_stream")
 
-    KERNELS = ("mask", "flux", "stage2")
+    KERNELS = ("mask", "flux", "stage2", "erosion")
 
     def profile(self, enable=True):
         return self._check(self.lib.imex_gpu_profile(self._h, int(bool(enable))), "profile")
 
     def kernel_times(self):
         """{kernel: (total_ms, launches)} since the last call (profile on)."""
-        ms = (C.c_double * 3)()
-        n = (C.c_int64 * 3)()
-        self._check(self.lib.imex_gpu_kernel_times(self._h, ms, n, 3), "kernel_times")
+        nk = len(self.KERNELS)
+        ms = (C.c_double * nk)()
+        n = (C.c_int64 * nk)()
+        self._check(self.lib.imex_gpu_kernel_times(self._h, ms, n, nk), "kernel_times")
         return {k: (ms[i], n[i]) for i, k in enumerate(self.KERNELS)}
 
     def device_state(self):

@@ -236,11 +236,12 @@ int imex_gpu_set_stream(ImexCtx* ctx, void* stream);
 int imex_gpu_device_state(ImexCtx* ctx, double** q_dev, int64_t* pitch);
 
 /* Measurement helpers (no counterpart in the reference).
- * imex_gpu_profile(ctx, 1) records CUDA events around the mask, flux and
- * stage-2 kernels that imex_gpu_advance launches without a graph, on the
- * context stream; imex_gpu_kernel_times returns, per kernel id (0 mask,
- * 1 flux, 2 stage 2), the summed event time in ms and the launch count since
- * the last call.  imex_gpu_measure_fp64_peak times an FP64 FMA-chain kernel
+ * imex_gpu_profile(ctx, 1) records CUDA events around the mask, flux,
+ * stage-2 and erosion/deposition kernels that imex_gpu_advance launches
+ * without a graph, on the context stream; imex_gpu_kernel_times returns, per
+ * kernel id (0 mask, 1 flux, 2 stage 2, 3 erosion/deposition; n_kernels must
+ * be at least 4), the summed event time in ms and the launch count since the
+ * last call.  imex_gpu_measure_fp64_peak times an FP64 FMA-chain kernel
  * and returns the achieved GFLOP/s (2 flops per FMA). */
 int imex_gpu_profile(ImexCtx* ctx, int enable);
 int imex_gpu_kernel_times(ImexCtx* ctx, double* total_ms, int64_t* launches, int n_kernels);
