@@ -85,11 +85,14 @@ IMEX_HD double fmax_f(double a, double b) {
 // oracle and the CUDA path evaluate it with this same sequence of IEEE
 // operations, so the two agree bit for bit; the sequence is
 //   log x = e*ln2 + 2*atanh(s), s = (m-1)/(m+1), m in [sqrt(1/2), sqrt(2)),
-//           atanh by its odd Taylor series to s^23,
-//   z = y*log x carried as an unevaluated sum of two doubles (Dekker's exact
-//       product with Veltkamp splitting, Knuth's two-sum),
+//           atanh by its odd Taylor series to s^23 (Horner with fused
+//           multiply-adds),
+//   z = y*log x carried as an unevaluated sum of two doubles (exact product
+//       error by one fused multiply-add, Knuth's two-sum),
 //   exp z = 2^k * exp(r), r = z - k*ln2 (ln2 split in two), exp(r) by its
-//           Taylor series to r^17.
+//           Taylor series to r^14 (Horner with fused multiply-adds).
+// Every fused multiply-add is the IEEE single-rounding operation on both
+// sides (CUDA fma, C++ std::fma), so the bits stay identical.
 // Accuracy against the exact power: within 4 ulp (measured); the reference's
 // libm pow is within 1 ulp, so results differ from it at that level only.
 IMEX_HD void two_sum(double a, double b, double& s, double& e) {
@@ -99,11 +102,7 @@ IMEX_HD void two_sum(double a, double b, double& s, double& e) {
 }
 IMEX_HD void two_prod(double a, double b, double& p, double& e) {
   p = a * b;
-  double c = 134217729.0 * a;
-  double ah = c - (c - a), al = a - ah;
-  c = 134217729.0 * b;
-  double bh = c - (c - b), bl = b - bh;
-  e = ((ah * bh - p) + ah * bl + al * bh) + al * bl;
+  e = fma(a, b, -p);
 }
 IMEX_NOINL double ipow(double x, double y) {
   if (isnan(x) || isnan(y)) return x + y;
@@ -128,15 +127,15 @@ IMEX_NOINL double ipow(double x, double y) {
                                      0x1.1111111111111p-4, 0x1.e1e1e1e1e1e1ep-5, 0x1.af286bca1af28p-5,
                                      0x1.8618618618618p-5, 0x1.642c8590b2164p-5};
   double P = inv_odd[10];
-  for (int k = 9; k >= 0; --k) P = inv_odd[k] + s2 * P;
+  for (int k = 9; k >= 0; --k) P = fma(s2, P, inv_odd[k]);
   double ts = 2.0 * s;
-  double logm = ts + ts * (s2 * P);
+  double logm = fma(ts, s2 * P, ts);
   double hi, lo;
   two_sum((double)e * LN2_HI, logm, hi, lo);
   lo = lo + (double)e * LN2_LO;
   double p, pe;
   two_prod(y, hi, p, pe);
-  pe = pe + y * lo;
+  pe = fma(y, lo, pe);
   double zh, zl;
   two_sum(p, pe, zh, zl);
   if (zh > 709.78) return __longlong_as_double(0x7ff0000000000000LL);
@@ -144,15 +143,14 @@ IMEX_NOINL double ipow(double x, double y) {
   double kf = rint(zh * INV_LN2);
   double rh, rl;
   two_sum(zh, -(kf * LN2_HI), rh, rl);
-  double r = rh + (rl + (zl - kf * LN2_LO));
-  const double fact[18] = {0x1.0000000000000p+0, 0x1.0000000000000p+0, 0x1.0000000000000p-1,
+  double r = rh + (rl + fma(-kf, LN2_LO, zl));
+  const double fact[15] = {0x1.0000000000000p+0, 0x1.0000000000000p+0, 0x1.0000000000000p-1,
                                   0x1.5555555555555p-3, 0x1.5555555555555p-5, 0x1.1111111111111p-7,
                                   0x1.6c16c16c16c17p-10, 0x1.a01a01a01a01ap-13, 0x1.a01a01a01a01ap-16,
                                   0x1.71de3a556c734p-19, 0x1.27e4fb7789f5cp-22, 0x1.ae64567f544e4p-26,
-                                  0x1.1eed8eff8d898p-29, 0x1.6124613a86d09p-33, 0x1.93974a8c07c9dp-37,
-                                  0x1.ae7f3e733b81fp-41, 0x1.ae7f3e733b81fp-45, 0x1.952c77030ad4ap-49};
-  double E = fact[17];
-  for (int k = 16; k >= 0; --k) E = fact[k] + r * E;
+                                  0x1.1eed8eff8d898p-29, 0x1.6124613a86d09p-33, 0x1.93974a8c07c9dp-37};
+  double E = fact[14];
+  for (int k = 13; k >= 0; --k) E = fma(r, E, fact[k]);
   return ldexp(E, (int)kf);
 }
 
@@ -637,27 +635,50 @@ IMEX_HD void implicit_terms_r(const DevParams& P, double bx, double by, const do
 }
 
 // --------------------------------------------- implicit terms (complex)
+// The complex-step Jacobian perturbs only q(2) or q(3), so every mixture
+// quantity built from q(1) and the solid loads alone (1/q1, mass fractions,
+// c_p, gas constant and 1/rho of the mixture's solid part) is the same for
+// both columns.  It is evaluated once per Newton iteration (CPrefix) and
+// shared; the operations, and so the values, are those of c_phys_var.
+template <int NS>
+struct CPrefix {
+  cplx inv, xc, spm, sgc, dot2;
+};
+
+template <int NS>
+IMEX_NOINL void implicit_prefix_c(const DevParams& P, const cplx* q, CPrefix<NS>& pre) {
+  if (!P.rheology_flag || !(q[0].re > EPS)) return;
+  cplx inv = rdiv(1.0, q[0]);
+  cplx xs[NS];
+#pragma unroll
+  for (int i = 0; i < NS; ++i) xs[i] = q[4 + i] * inv;
+  cplx xs_tot = C(0.0);
+#pragma unroll
+  for (int i = 0; i < NS; ++i) xs_tot = xs_tot + xs[i];
+  cplx xc = rsub(1.0, xs_tot);
+  cplx spc = (mulr(xc - C(0.0), P.sp_heat_a) + C(0.0)) / xc;
+  cplx dot = C(0.0);
+#pragma unroll
+  for (int i = 0; i < NS; ++i) dot = dot + mulr(conj(xs[i]), P.sp_heat_s[i]);
+  pre.spm = dot + xc * spc;
+  pre.sgc = (mulr(xc - C(0.0), P.sp_gas_const_a) + C(0.0)) / xc;
+  cplx dot2 = C(0.0);
+#pragma unroll
+  for (int i = 0; i < NS; ++i) dot2 = dot2 + conj(xs[i]) * C(P.inv_rho_s[i], 0.0);
+  pre.dot2 = dot2;
+  pre.inv = inv;
+  pre.xc = xc;
+}
+
 template <int NS>
 IMEX_NOINL void implicit_terms_c(const DevParams& P, double bx, double by, const cplx* q,
-                                 cplx& nh2, cplx& nh3) {
+                                 const CPrefix<NS>& pre, cplx& nh2, cplx& nh3) {
   nh2 = C(0.0, 0.0);
   nh3 = C(0.0, 0.0);
   if (!P.rheology_flag) return;
   cplx rho_m, u, v;
   if (q[0].re > EPS) {
-    cplx inv = rdiv(1.0, q[0]);
-    cplx xs[NS];
-#pragma unroll
-    for (int i = 0; i < NS; ++i) xs[i] = q[4 + i] * inv;
-    cplx xs_tot = C(0.0);
-#pragma unroll
-    for (int i = 0; i < NS; ++i) xs_tot = xs_tot + xs[i];
-    cplx xc = rsub(1.0, xs_tot);
-    cplx spc = (mulr(xc - C(0.0), P.sp_heat_a) + C(0.0)) / xc;
-    cplx dot = C(0.0);
-#pragma unroll
-    for (int i = 0; i < NS; ++i) dot = dot + mulr(conj(xs[i]), P.sp_heat_s[i]);
-    cplx spm = dot + xc * spc;
+    const cplx inv = pre.inv, xc = pre.xc, spm = pre.spm;
     cplx T;
     if (q[0].re > P.eps_sing) {
       if (P.energy_flag)
@@ -668,12 +689,8 @@ IMEX_NOINL void implicit_terms_c(const DevParams& P, double bx, double by, const
     } else {
       T = C(P.T_ambient);
     }
-    cplx sgc = (mulr(xc - C(0.0), P.sp_gas_const_a) + C(0.0)) / xc;
-    cplx irc = mulr(sgc * T, P.inv_pres);
-    cplx dot2 = C(0.0);
-#pragma unroll
-    for (int i = 0; i < NS; ++i) dot2 = dot2 + conj(xs[i]) * C(P.inv_rho_s[i], 0.0);
-    cplx irm = dot2 + xc * irc;
+    cplx irc = mulr(pre.sgc * T, P.inv_pres);
+    cplx irm = pre.dot2 + xc * irc;
     rho_m = rdiv(1.0, irm);
     if (q[0].re > P.eps_sing) {
       u = q[1] * inv;
@@ -708,7 +725,6 @@ IMEX_NOINL void implicit_terms_c(const DevParams& P, double bx, double by, const
   }
 }
 
-// ---------------------------------------- semi-implicit (Coulomb) terms
 template <int NS>
 IMEX_HD void semi_impl_terms(const DevParams& P, double bx, double by, double bxx,
                              double bxy, double byy, double gcf, const double* qpj,

@@ -39,6 +39,9 @@ struct ImexCtx {
   DevClock* clk = nullptr;
   DevClock* clk_host = nullptr;  // pinned mirror
   double* scratch = nullptr;     // AoS staging for transfers
+  NewtonWork nw{};               // stage-2 Newton state between passes
+  double* nw_buf = nullptr;      // backing store of nw's FP64 planes
+  uint32_t* nw_lists = nullptr;  // backing store of nw's three cell lists
   size_t scratch_bytes = 0;
   bool x_valid = false;          // X holds the fluxes of the current state
   bool exchange = false;         // erosion/deposition planes present
@@ -123,11 +126,23 @@ cudaError_t launch_flux(ImexCtx* ctx) {
 template <int NS>
 cudaError_t launch_stage2_ns(ImexCtx* ctx) {
   const DevParams& P = ctx->P;
-  int grid = grid_1d((long long)P.nx * P.ny, 128);
-  k_stage2<NS><<<grid, 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->X, ctx->mask, ctx->cellinfo,
-                                              ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy, ctx->Byy,
-                                              ctx->gc, ctx->clk);
-  ctx->launches += 1;
+  const long long ncell = (long long)P.nx * P.ny;
+  const int grid = grid_1d(ncell, STAGE2_THREADS);
+  // list passes: one resident wave (IMEX_STAGE2_MINB blocks per SM), grid-stride
+  const int lgrid = std::min(grid, 148 * IMEX_STAGE2_MINB);
+  k_nw_reset<<<1, 1, 0, ctx->stream>>>(ctx->clk);
+  k_stage2_first<NS><<<grid, STAGE2_THREADS, 0, ctx->stream>>>(
+      ctx->dP, ctx->q, ctx->X, ctx->mask, ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy, ctx->Byy, ctx->gc,
+      ctx->nw, ctx->clk);
+  k_stage2_iter<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->Bx, ctx->By,
+                                                               ctx->nw, ctx->clk, 2);
+  k_stage2_iter<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->Bx, ctx->By,
+                                                               ctx->nw, ctx->clk, 3);
+  k_stage2_tail<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->Bx, ctx->By,
+                                                               ctx->nw, ctx->clk);
+  k_stage2_post<NS><<<grid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->mask,
+                                                              ctx->cellinfo, ctx->nw, ctx->clk);
+  ctx->launches += 6;
   return cudaGetLastError();
 }
 
@@ -433,6 +448,10 @@ int imex_gpu_create(const ImexParams* p, const ImexStatic* s, int device, ImexCt
   }
 
   const size_t plane = (size_t)P.plane;
+  if (plane > (size_t)UINT32_MAX) {
+    delete ctx;
+    return IMEX_EUNSUPPORTED;  // stage-2 cell lists hold 32-bit plane indices
+  }
   CK(dalloc(&ctx->q, plane * nv));
   CK(dalloc(&ctx->X, plane * nv));
   CK(dalloc(&ctx->mask, plane));
@@ -496,6 +515,16 @@ int imex_gpu_create(const ImexParams* p, const ImexStatic* s, int device, ImexCt
   CK(cudaMemcpy(ctx->clk, ctx->clk_host, sizeof(DevClock), cudaMemcpyHostToDevice));
   ctx->scratch_bytes = N * (size_t)(nv + 2) * sizeof(double);
   CK(cudaMalloc((void**)&ctx->scratch, ctx->scratch_bytes));
+  // stage-2 Newton state: q_si, Rj, iterate, residual (nv planes each), |r|^2/2
+  CK(dalloc(&ctx->nw_buf, plane * (4 * (size_t)nv + 1)));
+  CK(dalloc(&ctx->nw.status, plane));
+  CK(dalloc(&ctx->nw_lists, plane * 3));
+  ctx->nw.qsi = ctx->nw_buf;
+  ctx->nw.Rj = ctx->nw_buf + plane * nv;
+  ctx->nw.x = ctx->nw_buf + plane * nv * 2;
+  ctx->nw.rt = ctx->nw_buf + plane * nv * 3;
+  ctx->nw.sf = ctx->nw_buf + plane * nv * 4;
+  for (int i = 0; i < 3; ++i) ctx->nw.list[i] = ctx->nw_lists + plane * i;
   CK(cudaDeviceSynchronize());
   *out = ctx;
   return IMEX_OK;
@@ -509,7 +538,8 @@ int imex_gpu_destroy(ImexCtx* ctx) {
   if (ctx->graph) cudaGraphDestroy(ctx->graph);
   void* bufs[] = {ctx->q, ctx->X, ctx->mask, ctx->cellinfo, ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy,
                   ctx->Byy, ctx->gc, ctx->dgc, ctx->gcsx, ctx->gcsy, ctx->release, ctx->erodible,
-                  ctx->deposit, ctx->erosion, ctx->Bcent, ctx->ring, ctx->clk, ctx->scratch, ctx->dP};
+                  ctx->deposit, ctx->erosion, ctx->Bcent, ctx->ring, ctx->clk, ctx->scratch, ctx->dP,
+                  ctx->nw_buf, ctx->nw.status, ctx->nw_lists};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (ctx->clk_host) cudaFreeHost(ctx->clk_host);

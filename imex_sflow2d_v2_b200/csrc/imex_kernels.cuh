@@ -7,8 +7,9 @@
 //               boundary/inlet rules, local speeds, Kurganov-Tadmor fluxes,
 //               divergence, explicit terms and the CFL minimum
 //               (timestep + RK stage 1: src/solver_2d.f90:872-1005,2614-3918)
-//   k_stage2    RK stage 2 per cell: semi-implicit terms, Newton with line
-//               search and complex-step Jacobian, assembly checks
+//   k_stage2_*  RK stage 2: semi-implicit terms, Newton with line search and
+//               complex-step Jacobian (one pass per Newton iteration over the
+//               cells still iterating), assembly checks
 //               (src/solver_2d.f90:1105-1628, 1660-2365)
 //   k_erosion   the erosion/deposition update per cell
 //               (src/solver_2d.f90:2380-2595)
@@ -53,6 +54,7 @@ struct DevClock {
   unsigned long long hist[16];
   unsigned long long solve_cells;
   unsigned long long steps;
+  unsigned int nw_count[4];  // cells appended to the stage-2 Newton lists
 };
 
 IMEX_HD double x_stag(const DevParams& P, int J) { return P.x0 + (double)(J - 1) * P.dx; }
@@ -582,12 +584,15 @@ __global__ void __launch_bounds__(FLUX_THREADS, IMEX_FLUX_MINB)
 }
 
 // =============================================================== Newton
-// solve_rk_step for a_diag = 1 (stage 2 of the n_RK = 2 tableau).
-template <int NS>
-struct NewtonOut {
-  int iters;
-  long long trials;
-};
+// solve_rk_step (src/solver_2d.f90:1660-1994) for a_diag = 1 (stage 2 of the
+// n_RK = 2 tableau), cut at its iteration boundaries: newton_start (scaling
+// and the test before the first iteration), newton_iter1 (the first
+// iteration, a full step) and newton_iterk (every later iteration, with the
+// line search).  The stage-2 passes below run one iteration per pass over a
+// compacted list of the cells still iterating; each cell goes through
+// exactly the operation sequence of one uninterrupted solve_rk_step.
+constexpr int NEWTON_MAX_IT = 100;
+constexpr double NEWTON_TOLF = 1.0e-10, NEWTON_STPMX = 100.0;
 
 template <int NS>
 __device__ __noinline__ void eval_f(const DevParams& P, const double* qj, const double* qj_old,
@@ -609,190 +614,226 @@ __device__ __noinline__ void eval_f(const DevParams& P, const double* qj, const 
   scal_f = 0.5 * d;
 }
 
+// Jacobian columns 2,3 by complex step (src/solver_2d.f90:2300-2365) and the
+// Newton direction: explicit rows diagonal, 2x2 Cramer on rows/cols 2,3
+// (src/solver_2d.f90:1879-1901).
 template <int NS>
-__device__ NewtonOut<NS> solve_rk_step(const DevParams& P, double* qj, const double* qj_old,
-                                       const double* Rj, double bx, double by, double dt) {
+__device__ __noinline__ void newton_direction(const DevParams& P, double bx, double by, double dt,
+                                              const double* qj_org, const double* qj_rel,
+                                              const double* rt, double* dd, double* J2,
+                                              double* J3) {
   constexpr int NV = 4 + NS;
-  const double TOLF = 1.0e-10, STPMX = 100.0;
-  double qj_org[NV], qj_rel[NV], rt[NV], x_old[NV], dd[NV];
-  double scal_f = 0.0;
-  long long trials = 0;
+  CPrefix<NS> pre;
+  {
+    cplx qc[NV];
+#pragma unroll
+    for (int m = 0; m < NV; ++m) qc[m] = mulr(C(qj_rel[m], 0.0), qj_org[m]);
+    implicit_prefix_c<NS>(P, qc, pre);
+  }
+#pragma unroll 1
+  for (int col = 1; col <= 2; ++col) {
+    cplx qc[NV];
+#pragma unroll
+    for (int m = 0; m < NV; ++m) qc[m] = mulr(C(qj_rel[m], (m == col) ? P.hstep : 0.0), qj_org[m]);
+    cplx nh2, nh3;
+    implicit_terms_c<NS>(P, bx, by, qc, pre, nh2, nh3);
+    double* Lc = (col == 1) ? J2 : J3;
+#pragma unroll
+    for (int r = 0; r < NV; ++r) {
+      double nim = (r == 1) ? nh2.im : ((r == 2) ? nh3.im : 0.0);
+      double jac = 1.0 * nim * P.one_by_h;
+      double l0 = (r == col) ? 1.0 * qj_org[col] : 0.0;
+      Lc[r] = l0 - dt * 1.0 * jac;
+    }
+  }
+  double d1[NV];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) d1[i] = (i == 1 || i == 2) ? 0.0 : rt[i] / (1.0 * qj_org[i]);
+  double d2a = rt[1], d2b = rt[2];
+  {
+    double s = 0.0, s2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+      if (i != 1 && i != 2) s += d1[i] * 0.0;
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+      if (i != 1 && i != 2) s2 += d1[i] * 0.0;
+    d2a = d2a - s;
+    d2b = d2b - s2;
+  }
+  double s11 = J2[1], s21 = J2[2], s12 = J3[1], s22 = J3[2];
+  double inv_det = 1.0 / (s11 * s22 - s21 * s12);
+  double sol0 = (d2a * s22 - d2b * s12) * inv_det;
+  double sol1 = (s11 * d2b - s21 * d2a) * inv_det;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    if (i == 1) dd[i] = -sol0 + 0.0;
+    else if (i == 2) dd[i] = -sol1 + 0.0;
+    else dd[i] = 0.0 + (-d1[i]);
+  }
+}
+
+// The exit tests at the end of an iteration (src/solver_2d.f90:1964-1988).
+template <int NS>
+__device__ __forceinline__ bool newton_converged(const double* rt, const double* qj_rel,
+                                                 const double* x_old) {
+  constexpr int NV = 4 + NS;
+  double mx = fabs(rt[0]);
+#pragma unroll
+  for (int i = 1; i < NV; ++i) mx = fmax_f(mx, fabs(rt[i]));
+  if (mx < NEWTON_TOLF) return true;
+  double m3 = 0.0;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    double r = fabs(qj_rel[i] - x_old[i]) / fmax_f(fabs(qj_rel[i]), 1.0);
+    m3 = (i == 0) ? r : fmax_f(m3, r);
+  }
+  return m3 < EPS;
+}
+
+// Scaling (src/solver_2d.f90:1786-1798); the residual test before the first
+// Jacobian.  True: q already satisfies TOLF (exit with nl_iter = 1).
+template <int NS>
+__device__ __forceinline__ void newton_scale(const double* qj, double* qj_org) {
+  constexpr int NV = 4 + NS;
 #pragma unroll
   for (int i = 0; i < NV; ++i) qj_org[i] = fmax_f(fabs(qj[i]), 1.0e-3);
+}
+
+template <int NS>
+__device__ bool newton_start(const DevParams& P, const double* qj, const double* qj_old,
+                             const double* Rj, double bx, double by, double dt,
+                             const double* qj_org, double* qj_rel, double* rt, double& scal_f) {
+  constexpr int NV = 4 + NS;
 #pragma unroll
   for (int i = 0; i < NV; ++i) qj_rel[i] = qj[i] / qj_org[i];
-  int nl_iter;
-  for (nl_iter = 1; nl_iter <= 100; ++nl_iter) {
-    if (nl_iter == 1) {
-      eval_f<NS>(P, qj, qj_old, Rj, bx, by, dt, rt, scal_f);
-      double mx = fabs(rt[0]);
+  eval_f<NS>(P, qj, qj_old, Rj, bx, by, dt, rt, scal_f);
+  double mx = fabs(rt[0]);
 #pragma unroll
-      for (int i = 1; i < NV; ++i) mx = fmax_f(mx, fabs(rt[i]));
-      if (mx < TOLF) break;
+  for (int i = 1; i < NV; ++i) mx = fmax_f(mx, fabs(rt[i]));
+  return mx < NEWTON_TOLF;
+}
+
+// Iteration 1: full Newton step, no line search.  qj receives the iterate.
+template <int NS>
+__device__ bool newton_iter1(const DevParams& P, double* qj, const double* qj_old,
+                             const double* Rj, double bx, double by, double dt,
+                             const double* qj_org, double* qj_rel, double* rt, double& scal_f) {
+  constexpr int NV = 4 + NS;
+  double dd[NV], J2[NV], J3[NV], x_old[NV];
+  newton_direction<NS>(P, bx, by, dt, qj_org, qj_rel, rt, dd, J2, J3);
+#pragma unroll
+  for (int i = 0; i < NV; ++i) x_old[i] = qj_rel[i];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i] + dd[i];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) qj[i] = qj_rel[i] * qj_org[i];
+  eval_f<NS>(P, qj, qj_old, Rj, bx, by, dt, rt, scal_f);
+#pragma unroll
+  for (int i = 0; i < NV; ++i) qj[i] = qj_rel[i] * qj_org[i];
+  return newton_converged<NS>(rt, qj_rel, x_old);
+}
+
+// Iterations 2..100: Newton direction and lnsrch (src/solver_2d.f90:
+// 1929-1962, 2019-2224).  Every backtrack after the first halves alam: the
+// cubic model's value is clamped to <= alam/2 and then maxed with alam/2.
+// The trials are capped at 4096; the cap exits like alam < alamin.
+template <int NS>
+__device__ __noinline__ bool newton_iterk(const DevParams& P, double* qj, const double* qj_old,
+                                          const double* Rj, double bx, double by, double dt,
+                                          const double* qj_org, double* qj_rel, double* rt,
+                                          double& scal_f, long long& trials) {
+  constexpr int NV = 4 + NS;
+  double dd[NV], J2[NV], J3[NV], x_old[NV];
+  newton_direction<NS>(P, bx, by, dt, qj_org, qj_rel, rt, dd, J2, J3);
+#pragma unroll
+  for (int i = 0; i < NV; ++i) x_old[i] = qj_rel[i];
+  const double scal_f_old = scal_f;
+  double sdot = 0.0;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) sdot += qj_rel[i] * qj_rel[i];
+  double stpmax = NEWTON_STPMX * fmax_f(sqrt(sdot), (double)NV);
+  double grad[NV];
+#pragma unroll
+  for (int c = 0; c < NV; ++c) {
+    double s = 0.0;
+#pragma unroll
+    for (int r = 0; r < NV; ++r) {
+      double L;
+      if (c == 1) L = J2[r];
+      else if (c == 2) L = J3[r];
+      else L = (r == c) ? 1.0 * qj_org[c] : 0.0;
+      s += rt[r] * L;
     }
-    // Jacobian columns 2,3 by complex step (src/solver_2d.f90:2300-2365)
-    double J2[NV], J3[NV];  // left_matrix(:,2), left_matrix(:,3)
-#pragma unroll 1
-    for (int col = 1; col <= 2; ++col) {
-      cplx qc[NV];
+    grad[c] = s;
+  }
+  double scale = 0.0, ssq = 0.0;
 #pragma unroll
-      for (int m = 0; m < NV; ++m) qc[m] = mulr(C(qj_rel[m], (m == col) ? P.hstep : 0.0), qj_org[m]);
-      cplx nh2, nh3;
-      implicit_terms_c<NS>(P, bx, by, qc, nh2, nh3);
-      double* Lc = (col == 1) ? J2 : J3;
-#pragma unroll
-      for (int r = 0; r < NV; ++r) {
-        double nim = (r == 1) ? nh2.im : ((r == 2) ? nh3.im : 0.0);
-        double jac = 1.0 * nim * P.one_by_h;
-        double l0 = (r == col) ? 1.0 * qj_org[col] : 0.0;
-        Lc[r] = l0 - dt * 1.0 * jac;
+  for (int i = 0; i < NV; ++i) {
+    if (dd[i] != 0.0) {
+      double ax = fabs(dd[i]);
+      if (scale < ax) {
+        double val = scale / ax;
+        ssq = 1.0 + ssq * val * val;
+        scale = ax;
+      } else {
+        double val = ax / scale;
+        ssq = ssq + val * val;
       }
     }
-    // block elimination: explicit rows diagonal, 2x2 Cramer on rows/cols 2,3
-    double d1[NV];
+  }
+  double dabs = scale * sqrt(ssq);
+  if (dabs > stpmax) {
 #pragma unroll
-    for (int i = 0; i < NV; ++i) d1[i] = (i == 1 || i == 2) ? 0.0 : rt[i] / (1.0 * qj_org[i]);
-    double d2a = rt[1], d2b = rt[2];
-    {
-      double s = 0.0, s2 = 0.0;
+    for (int i = 0; i < NV; ++i) dd[i] = dd[i] * stpmax / dabs;
+  }
+  double slope = 0.0;
 #pragma unroll
-      for (int i = 0; i < NV; ++i)
-        if (i != 1 && i != 2) {
-          s += d1[i] * 0.0;
-        }
+  for (int i = 0; i < NV; ++i) slope += grad[i] * dd[i];
+  double mx = 0.0;
 #pragma unroll
-      for (int i = 0; i < NV; ++i)
-        if (i != 1 && i != 2) {
-          s2 += d1[i] * 0.0;
-        }
-      d2a = d2a - s;
-      d2b = d2b - s2;
-    }
-    double s11 = J2[1], s21 = J2[2], s12 = J3[1], s22 = J3[2];
-    double inv_det = 1.0 / (s11 * s22 - s21 * s12);
-    double sol0 = (d2a * s22 - d2b * s12) * inv_det;
-    double sol1 = (s11 * d2b - s21 * d2a) * inv_det;
+  for (int i = 0; i < NV; ++i) {
+    double r = fabs(dd[i]) / fmax_f(fabs(x_old[i]), 1.0);
+    mx = (i == 0) ? r : fmax_f(mx, r);
+  }
+  double alamin = EPS / mx;
+  if (alamin == 0.0) {
 #pragma unroll
-    for (int i = 0; i < NV; ++i) {
-      if (i == 1) dd[i] = -sol0 + 0.0;
-      else if (i == 2) dd[i] = -sol1 + 0.0;
-      else dd[i] = 0.0 + (-d1[i]);
-    }
+    for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i];
+  } else {
+    double alam = 1.0;
+    int trial;
+    for (trial = 0; trial < 4096; ++trial) {
+      double qt[NV];
 #pragma unroll
-    for (int i = 0; i < NV; ++i) x_old[i] = qj_rel[i];
-    const double scal_f_old = scal_f;
-    if (nl_iter > 1) {
-      double sdot = 0.0;
+      for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i] + alam * dd[i];
 #pragma unroll
-      for (int i = 0; i < NV; ++i) sdot += qj_rel[i] * qj_rel[i];
-      double stpmax = STPMX * fmax_f(sqrt(sdot), (double)NV);
-      double grad[NV];
-#pragma unroll
-      for (int c = 0; c < NV; ++c) {
-        double s = 0.0;
-#pragma unroll
-        for (int r = 0; r < NV; ++r) {
-          double L;
-          if (c == 1) L = J2[r];
-          else if (c == 2) L = J3[r];
-          else L = (r == c) ? 1.0 * qj_org[c] : 0.0;
-          s += rt[r] * L;
-        }
-        grad[c] = s;
-      }
-      // lnsrch (src/solver_2d.f90:2019-2224)
-      double scale = 0.0, ssq = 0.0;
-#pragma unroll
-      for (int i = 0; i < NV; ++i) {
-        if (dd[i] != 0.0) {
-          double ax = fabs(dd[i]);
-          if (scale < ax) {
-            double val = scale / ax;
-            ssq = 1.0 + ssq * val * val;
-            scale = ax;
-          } else {
-            double val = ax / scale;
-            ssq = ssq + val * val;
-          }
-        }
-      }
-      double dabs = scale * sqrt(ssq);
-      if (dabs > stpmax) {
-#pragma unroll
-        for (int i = 0; i < NV; ++i) dd[i] = dd[i] * stpmax / dabs;
-      }
-      double slope = 0.0;
-#pragma unroll
-      for (int i = 0; i < NV; ++i) slope += grad[i] * dd[i];
-      double mx = 0.0;
-#pragma unroll
-      for (int i = 0; i < NV; ++i) {
-        double r = fabs(dd[i]) / fmax_f(fabs(x_old[i]), 1.0);
-        mx = (i == 0) ? r : fmax_f(mx, r);
-      }
-      double alamin = EPS / mx;
-      if (alamin == 0.0) {
+      for (int i = 0; i < NV; ++i) qt[i] = qj_rel[i] * qj_org[i];
+      eval_f<NS>(P, qt, qj_old, Rj, bx, by, dt, rt, scal_f);
+      ++trials;
+      if (scal_f <= 0.9 * scal_f_old) break;
+      if (alam < alamin) {
 #pragma unroll
         for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i];
-      } else {
-        double alam = 1.0;
-        // every backtrack after the first halves alam: the cubic model's
-        // value is clamped to <= alam/2 and then maxed with alam/2.  The
-        // trials are capped at 4096; the cap exits like alam < alamin.
-        int trial;
-        for (trial = 0; trial < 4096; ++trial) {
-          double qt[NV];
-#pragma unroll
-          for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i] + alam * dd[i];
-#pragma unroll
-          for (int i = 0; i < NV; ++i) qt[i] = qj_rel[i] * qj_org[i];
-          eval_f<NS>(P, qt, qj_old, Rj, bx, by, dt, rt, scal_f);
-          ++trials;
-          if (scal_f <= 0.9 * scal_f_old) break;
-          if (alam < alamin) {
-#pragma unroll
-            for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i];
-            scal_f = scal_f_old;
-            break;
-          }
-          if (alam == 1.0) {
-            double tmplam = -slope / (2.0 * (scal_f - scal_f_old - slope));
-            alam = fmax_f(tmplam, 0.5 * alam);
-          } else {
-            alam = 0.5 * alam;
-          }
-        }
-        if (trial == 4096) {
-#pragma unroll
-          for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i];
-          scal_f = scal_f_old;
-        }
+        scal_f = scal_f_old;
+        break;
       }
-    } else {
-#pragma unroll
-      for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i] + dd[i];
-#pragma unroll
-      for (int i = 0; i < NV; ++i) qj[i] = qj_rel[i] * qj_org[i];
-      eval_f<NS>(P, qj, qj_old, Rj, bx, by, dt, rt, scal_f);
+      if (alam == 1.0) {
+        double tmplam = -slope / (2.0 * (scal_f - scal_f_old - slope));
+        alam = fmax_f(tmplam, 0.5 * alam);
+      } else {
+        alam = 0.5 * alam;
+      }
     }
+    if (trial == 4096) {
 #pragma unroll
-    for (int i = 0; i < NV; ++i) qj[i] = qj_rel[i] * qj_org[i];
-    double mx = fabs(rt[0]);
-#pragma unroll
-    for (int i = 1; i < NV; ++i) mx = fmax_f(mx, fabs(rt[i]));
-    if (mx < TOLF) break;
-    double m3 = 0.0;
-#pragma unroll
-    for (int i = 0; i < NV; ++i) {
-      double r = fabs(qj_rel[i] - x_old[i]) / fmax_f(fabs(qj_rel[i]), 1.0);
-      m3 = (i == 0) ? r : fmax_f(m3, r);
+      for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i];
+      scal_f = scal_f_old;
     }
-    if (m3 < EPS) break;
   }
-  NewtonOut<NS> o;
-  o.iters = nl_iter > 100 ? 100 : nl_iter;
-  o.trials = trials;
-  return o;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) qj[i] = qj_rel[i] * qj_org[i];
+  return newton_converged<NS>(rt, qj_rel, x_old);
 }
 
 // ============================================================ mass exchange
@@ -960,104 +1001,334 @@ __device__ bool erosion_cell(const DevParams& P, double* qc, double bx, double b
   return bad;
 }
 
-// =============================================================== k_stage2
+// =============================================================== stage 2
+// RK stage 2 (src/solver_2d.f90:1105-1628) as passes over the solve cells:
+//   k_stage2_first   q_fv, semi-implicit terms, q_si, Rj_not_impl, Newton
+//                    scaling and iteration 1; cells that go on are appended
+//                    to list 0
+//   k_stage2_iter    one Newton iteration (nl_iter = 2 or 3) over a list;
+//                    cells that go on are appended to the next list
+//   k_stage2_tail    iterations 4..100 for the few cells still iterating
+//   k_stage2_post    sign guard, assemble_sol checks and fixes, q written
+// Between passes a cell's Newton state (qj_rel, the residual, its norm) is
+// kept in the NewtonWork planes; the iterate is carried bit for bit, so a
+// cell's arithmetic is that of one uninterrupted solve_rk_step.  Iteration
+// counts differ from cell to cell (mostly 2 or 3 here); running each
+// iteration as its own pass over the cells that need it keeps a warp's
+// lanes on the same iteration.
+struct NewtonWork {
+  double* qsi;    // nv planes: q_si, the Newton initial guess (scaling source)
+  double* Rj;     // nv planes: Rj_not_impl
+  double* x;      // nv planes: qj_rel while iterating, the final qj when done
+  double* rt;     // nv planes: residual
+  double* sf;     // 1 plane: 0.5*|residual|^2
+  uint8_t* status;  // 1 plane: 1 = the cell went through Newton
+  uint32_t* list[3];  // cells (k*pitch + j) still iterating after pass 0, 1, 2
+};
+
+constexpr int STAGE2_THREADS = 128;
+
+__device__ __forceinline__ void list_append(bool add, uint32_t c, uint32_t* list,
+                                            unsigned int* count) {
+  const unsigned m = __ballot_sync(0xffffffffu, add);
+  if (!m) return;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(m) - 1;
+  unsigned int base = 0;
+  if (lane == leader) base = atomicAdd(count, (unsigned int)__popc(m));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (add) list[base + __popc(m & ((1u << lane) - 1u))] = c;
+}
+
+// Newton statistics of the cells that finished in this warp iteration
+// (iters = 0: no cell finished in this lane).
+__device__ __forceinline__ void newton_finish_stats(DevClock* clk, int iters,
+                                                    unsigned long long& it_sum,
+                                                    unsigned long long& maxit) {
+  const int bin = iters > 0 ? (iters < 16 ? iters - 1 : 15) : -1;
+  const unsigned peers = __match_any_sync(0xffffffffu, bin);
+  if (bin >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1)
+    atomicAdd(&clk->hist[bin], (unsigned long long)__popc(peers));
+  if (iters > 0) {
+    it_sum += (unsigned long long)iters;
+    if (iters >= NEWTON_MAX_IT) maxit += 1;
+  }
+}
+
+__device__ __forceinline__ void newton_flush_stats(DevClock* clk, unsigned long long cells,
+                                                   unsigned long long it_sum,
+                                                   unsigned long long trials,
+                                                   unsigned long long maxit) {
+  for (int off = 16; off > 0; off >>= 1) {
+    cells += __shfl_down_sync(0xffffffffu, cells, off);
+    it_sum += __shfl_down_sync(0xffffffffu, it_sum, off);
+    trials += __shfl_down_sync(0xffffffffu, trials, off);
+    maxit += __shfl_down_sync(0xffffffffu, maxit, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (cells) atomicAdd(&clk->newton_cells, cells);
+    if (it_sum) atomicAdd(&clk->newton_iters, it_sum);
+    if (trials) atomicAdd(&clk->lnsrch_trials, trials);
+    if (maxit) atomicAdd(&clk->newton_maxit, maxit);
+  }
+}
+
 template <int NS>
-__global__ void __launch_bounds__(128, IMEX_STAGE2_MINB)
-    k_stage2(const DevParams* __restrict__ Pp, double* __restrict__ q, const double* __restrict__ X,
-             const uint8_t* __restrict__ mask, const uint8_t* __restrict__ cellinfo,
-             const double* __restrict__ Bx, const double* __restrict__ By,
-             const double* __restrict__ Bxx, const double* __restrict__ Bxy,
-             const double* __restrict__ Byy, const double* __restrict__ gc, DevClock* clk) {
+__global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
+    k_stage2_first(const DevParams* __restrict__ Pp, const double* __restrict__ q,
+                   const double* __restrict__ X, const uint8_t* __restrict__ mask,
+                   const double* __restrict__ Bx, const double* __restrict__ By,
+                   const double* __restrict__ Bxx, const double* __restrict__ Bxy,
+                   const double* __restrict__ Byy, const double* __restrict__ gc, NewtonWork W,
+                   DevClock* clk) {
+  const DevParams& P = *Pp;
+  constexpr int NV = 4 + NS, NP = 6 + NS;
+  const int nx = P.nx;
+  const long long ncell = (long long)nx * P.ny;
+  const size_t N = (size_t)P.plane;
+  const double dt = clk->dt;
+  unsigned long long cells = 0, it_sum = 0, maxit = 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < ncell;
+       base += stride) {
+    const long long g = base + (threadIdx.x & 31);
+    size_t c = 0;
+    bool go_on = false;
+    int fin = 0;
+    if (g < ncell) {
+      const int j = (int)(g % nx), k = (int)(g / nx);
+      c = (size_t)k * P.pitch + j;
+      if (mask[c]) {
+        double q0[NV], qfv[NV], Xc[NV];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+          q0[i] = q[c + i * N];
+          Xc[i] = X[c + i * N];
+        }
+        // q_fv = q0 - dt*(MATMUL(divFlux-expl, a_tilde) - MATMUL(NH+SI_NH, a_dirk))
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+          double sa = (0.0 + Xc[i] * 1.0) + (0.0 - 0.0) * 0.0;
+          double sb = (0.0 + (0.0 + 0.0) * 0.0) + (0.0 + 0.0) * 0.0;
+          qfv[i] = q0[i] - dt * (sa - sb);
+        }
+        double qg[NV];
+        if (qfv[0] > 0.0) {
+          double qpv[NP];
+          qc_to_qp<NS>(P, qfv, qpv);
+          const double bx = Bx[c], by = By[c];
+          double bxx = 0.0, bxy = 0.0, byy = 0.0, gcf = 1.0;
+          if (P.curvature_term_flag) {
+            bxx = Bxx[c];
+            bxy = Bxy[c];
+            byy = Byy[c];
+          }
+          if (P.slope_correction_flag) gcf = gc[c];
+          double si2, si3;
+          semi_impl_terms<NS>(P, bx, by, bxx, bxy, byy, gcf, qpv, si2, si3);
+          double SI[NV], qsi[NV];
+#pragma unroll
+          for (int i = 0; i < NV; ++i) SI[i] = (i == 1) ? si2 : ((i == 2) ? si3 : 0.0);
+#pragma unroll
+          for (int i = 0; i < NV; ++i) qsi[i] = qfv[i] + dt * 1.0 * SI[i];
+          if (qfv[1] * qfv[1] + qfv[2] * qfv[2] == 0.0) {
+            qsi[1] = 0.0;
+            qsi[2] = 0.0;
+          } else if (qsi[1] * qfv[1] < 0.0 || qsi[2] * qfv[2] < 0.0) {
+            qsi[1] = 0.0;
+            qsi[2] = 0.0;
+          } else {
+            double Sm = sqrt(qsi[1] * qsi[1] + qsi[2] * qsi[2]);
+            double Fm = sqrt(qfv[1] * qfv[1] + qfv[2] * qfv[2]);
+            qsi[1] = Sm * qfv[1] / Fm;
+            qsi[2] = Sm * qfv[2] / Fm;
+          }
+          double Rj[NV];
+#pragma unroll
+          for (int i = 0; i < NV; ++i) {
+            SI[i] = (qsi[i] - qfv[i]) / (dt * 1.0);
+            double sa = 0.0 + Xc[i] * 1.0;
+            double sb = 0.0 + (0.0 + 0.0) * 0.0;
+            Rj[i] = (sa - sb) - 1.0 * SI[i];
+            qg[i] = qsi[i];
+            W.qsi[c + i * N] = qsi[i];
+            W.Rj[c + i * N] = Rj[i];
+          }
+          W.status[c] = 1;
+          cells += 1;
+          double qj_org[NV], qj_rel[NV], rt[NV], scal_f;
+          newton_scale<NS>(qg, qj_org);
+          if (newton_start<NS>(P, qg, q0, Rj, bx, by, dt, qj_org, qj_rel, rt, scal_f)) {
+            fin = 1;
+          } else if (newton_iter1<NS>(P, qg, q0, Rj, bx, by, dt, qj_org, qj_rel, rt, scal_f)) {
+            fin = 1;
+          } else {
+            go_on = true;
+#pragma unroll
+            for (int i = 0; i < NV; ++i) {
+              W.x[c + i * N] = qj_rel[i];
+              W.rt[c + i * N] = rt[i];
+            }
+            W.sf[c] = scal_f;
+          }
+        } else {
+#pragma unroll
+          for (int i = 0; i < NV; ++i) qg[i] = qfv[i];
+          W.status[c] = 0;
+        }
+        if (!go_on) {
+#pragma unroll
+          for (int i = 0; i < NV; ++i) W.x[c + i * N] = qg[i];
+        }
+      }
+    }
+    newton_finish_stats(clk, fin, it_sum, maxit);
+    list_append(go_on, (uint32_t)c, W.list[0], &clk->nw_count[0]);
+  }
+  newton_flush_stats(clk, cells, it_sum, 0, maxit);
+}
+
+// One Newton iteration (nl_iter = 2 or 3) for the cells of list `in`.
+template <int NS>
+__global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
+    k_stage2_iter(const DevParams* __restrict__ Pp, const double* __restrict__ q,
+                  const double* __restrict__ Bx, const double* __restrict__ By, NewtonWork W,
+                  DevClock* clk, int nl_iter) {
+  const DevParams& P = *Pp;
+  constexpr int NV = 4 + NS;
+  const size_t N = (size_t)P.plane;
+  const double dt = clk->dt;
+  const uint32_t* in = W.list[nl_iter - 2];
+  uint32_t* out = W.list[nl_iter - 1];
+  const long long n = (long long)clk->nw_count[nl_iter - 2];
+  unsigned long long it_sum = 0, maxit = 0, trials = 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n;
+       base += stride) {
+    const long long e = base + (threadIdx.x & 31);
+    uint32_t c = 0;
+    bool go_on = false;
+    int fin = 0;
+    if (e < n) {
+      c = in[e];
+      double q0[NV], Rj[NV], qj_org[NV], qj_rel[NV], rt[NV], qj[NV], scal_f;
+#pragma unroll
+      for (int i = 0; i < NV; ++i) {
+        q0[i] = q[c + i * N];
+        Rj[i] = W.Rj[c + i * N];
+        qj[i] = W.qsi[c + i * N];
+        qj_rel[i] = W.x[c + i * N];
+        rt[i] = W.rt[c + i * N];
+      }
+      scal_f = W.sf[c];
+      newton_scale<NS>(qj, qj_org);
+      long long tr = 0;
+      bool done = newton_iterk<NS>(P, qj, q0, Rj, Bx[c], By[c], dt, qj_org, qj_rel, rt, scal_f, tr);
+      trials += (unsigned long long)tr;
+      if (done || nl_iter >= NEWTON_MAX_IT) {
+        fin = nl_iter;
+#pragma unroll
+        for (int i = 0; i < NV; ++i) W.x[c + i * N] = qj[i];
+      } else {
+        go_on = true;
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+          W.x[c + i * N] = qj_rel[i];
+          W.rt[c + i * N] = rt[i];
+        }
+        W.sf[c] = scal_f;
+      }
+    }
+    newton_finish_stats(clk, fin, it_sum, maxit);
+    list_append(go_on, c, out, &clk->nw_count[nl_iter - 1]);
+  }
+  newton_flush_stats(clk, 0, it_sum, trials, maxit);
+}
+
+// Iterations 4..100 for the cells of list 2.
+template <int NS>
+__global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
+    k_stage2_tail(const DevParams* __restrict__ Pp, const double* __restrict__ q,
+                  const double* __restrict__ Bx, const double* __restrict__ By, NewtonWork W,
+                  DevClock* clk) {
+  const DevParams& P = *Pp;
+  constexpr int NV = 4 + NS;
+  const size_t N = (size_t)P.plane;
+  const double dt = clk->dt;
+  const long long n = (long long)clk->nw_count[2];
+  unsigned long long it_sum = 0, maxit = 0, trials = 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n;
+       base += stride) {
+    const long long e = base + (threadIdx.x & 31);
+    int fin = 0;
+    if (e < n) {
+      const uint32_t c = W.list[2][e];
+      double q0[NV], Rj[NV], qj_org[NV], qj_rel[NV], rt[NV], qj[NV], scal_f;
+#pragma unroll
+      for (int i = 0; i < NV; ++i) {
+        q0[i] = q[c + i * N];
+        Rj[i] = W.Rj[c + i * N];
+        qj[i] = W.qsi[c + i * N];
+        qj_rel[i] = W.x[c + i * N];
+        rt[i] = W.rt[c + i * N];
+      }
+      scal_f = W.sf[c];
+      newton_scale<NS>(qj, qj_org);
+      const double bx = Bx[c], by = By[c];
+      int it;
+      for (it = 4; it <= NEWTON_MAX_IT; ++it) {
+        long long tr = 0;
+        bool done = newton_iterk<NS>(P, qj, q0, Rj, bx, by, dt, qj_org, qj_rel, rt, scal_f, tr);
+        trials += (unsigned long long)tr;
+        if (done) break;
+      }
+      fin = it > NEWTON_MAX_IT ? NEWTON_MAX_IT : it;
+#pragma unroll
+      for (int i = 0; i < NV; ++i) W.x[c + i * N] = qj[i];
+    }
+    newton_finish_stats(clk, fin, it_sum, maxit);
+  }
+  newton_flush_stats(clk, 0, it_sum, trials, maxit);
+}
+
+// Sign guard after Newton (src/solver_2d.f90:1238-1255) and assemble_sol
+// (src/solver_2d.f90:1339-1626).
+template <int NS>
+__global__ void __launch_bounds__(STAGE2_THREADS)
+    k_stage2_post(const DevParams* __restrict__ Pp, double* __restrict__ q,
+                  const uint8_t* __restrict__ mask, const uint8_t* __restrict__ cellinfo,
+                  NewtonWork W, DevClock* clk) {
   const DevParams& P = *Pp;
   constexpr int NV = 4 + NS, NP = 6 + NS;
   const int nx = P.nx, ny = P.ny;
   const long long ncell = (long long)nx * ny;
-  long long newton_cells = 0, newton_iters = 0, trials = 0, maxit = 0;
-  const double dt = clk->dt;
+  const size_t N = (size_t)P.plane;
   for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < ncell;
        g += (long long)gridDim.x * blockDim.x) {
-    int j = (int)(g % nx), k = (int)(g / nx);
-    size_t c = (size_t)k * P.pitch + j;
+    const int j = (int)(g % nx), k = (int)(g / nx);
+    const size_t c = (size_t)k * P.pitch + j;
     if (!mask[c]) continue;
-    double q0[NV], qfv[NV], Xc[NV];
+    double qc[NV];
 #pragma unroll
-    for (int i = 0; i < NV; ++i) {
-      q0[i] = q[c + (size_t)i * P.plane];
-      Xc[i] = X[c + (size_t)i * P.plane];
-    }
-    // q_fv = q0 - dt*(MATMUL(divFlux-expl, a_tilde) - MATMUL(NH+SI_NH, a_dirk))
-#pragma unroll
-    for (int i = 0; i < NV; ++i) {
-      double sa = (0.0 + Xc[i] * 1.0) + (0.0 - 0.0) * 0.0;
-      double sb = (0.0 + (0.0 + 0.0) * 0.0) + (0.0 + 0.0) * 0.0;
-      qfv[i] = q0[i] - dt * (sa - sb);
-    }
-    double qpv[NP];
-    qc_to_qp<NS>(P, qfv, qpv);
-    double qg[NV], qsi[NV];
-    const double bx = Bx[c], by = By[c];
-    if (qfv[0] > 0.0) {
-      double bxx = 0.0, bxy = 0.0, byy = 0.0, gcf = 1.0;
-      if (P.curvature_term_flag) {
-        bxx = Bxx[c];
-        bxy = Bxy[c];
-        byy = Byy[c];
-      }
-      if (P.slope_correction_flag) gcf = gc[c];
-      double si2, si3;
-      semi_impl_terms<NS>(P, bx, by, bxx, bxy, byy, gcf, qpv, si2, si3);
-      double SI[NV];
-#pragma unroll
-      for (int i = 0; i < NV; ++i) SI[i] = (i == 1) ? si2 : ((i == 2) ? si3 : 0.0);
-#pragma unroll
-      for (int i = 0; i < NV; ++i) qsi[i] = qfv[i] + dt * 1.0 * SI[i];
-      if (qfv[1] * qfv[1] + qfv[2] * qfv[2] == 0.0) {
-        qsi[1] = 0.0;
-        qsi[2] = 0.0;
-      } else if (qsi[1] * qfv[1] < 0.0 || qsi[2] * qfv[2] < 0.0) {
-        qsi[1] = 0.0;
-        qsi[2] = 0.0;
+    for (int i = 0; i < NV; ++i) qc[i] = W.x[c + i * N];
+    if (W.status[c]) {
+      const double qs1 = W.qsi[c + N], qs2 = W.qsi[c + 2 * N];
+      if (ny == 1) qc[2] = 0.0;
+      if (nx == 1) qc[1] = 0.0;
+      if (qs1 * qs1 + qs2 * qs2 == 0.0) {
+        qc[1] = 0.0;
+        qc[2] = 0.0;
+      } else if (qc[1] * qs1 <= 0.0 && qc[2] * qs2 <= 0.0) {
+        qc[1] = 0.0;
+        qc[2] = 0.0;
       } else {
-        double Sm = sqrt(qsi[1] * qsi[1] + qsi[2] * qsi[2]);
-        double Fm = sqrt(qfv[1] * qfv[1] + qfv[2] * qfv[2]);
-        qsi[1] = Sm * qfv[1] / Fm;
-        qsi[2] = Sm * qfv[2] / Fm;
+        double Sm = sqrt(qc[1] * qc[1] + qc[2] * qc[2]);
+        double Fm = sqrt(qs1 * qs1 + qs2 * qs2);
+        qc[1] = Sm * qs1 / Fm;
+        qc[2] = Sm * qs2 / Fm;
       }
-      double Rj[NV];
-#pragma unroll
-      for (int i = 0; i < NV; ++i) {
-        SI[i] = (qsi[i] - qfv[i]) / (dt * 1.0);
-        double sa = 0.0 + Xc[i] * 1.0;
-        double sb = 0.0 + (0.0 + 0.0) * 0.0;
-        Rj[i] = (sa - sb) - 1.0 * SI[i];
-        qg[i] = qsi[i];
-      }
-      NewtonOut<NS> no = solve_rk_step<NS>(P, qg, q0, Rj, bx, by, dt);
-      newton_cells += 1;
-      newton_iters += no.iters;
-      trials += no.trials;
-      if (no.iters >= 100) maxit += 1;
-      atomicAdd(&clk->hist[no.iters < 16 ? no.iters - 1 : 15], 1ULL);
-      if (ny == 1) qg[2] = 0.0;
-      if (nx == 1) qg[1] = 0.0;
-      if (qsi[1] * qsi[1] + qsi[2] * qsi[2] == 0.0) {
-        qg[1] = 0.0;
-        qg[2] = 0.0;
-      } else if (qg[1] * qsi[1] <= 0.0 && qg[2] * qsi[2] <= 0.0) {
-        qg[1] = 0.0;
-        qg[2] = 0.0;
-      } else {
-        double Sm = sqrt(qg[1] * qg[1] + qg[2] * qg[2]);
-        double Fm = sqrt(qsi[1] * qsi[1] + qsi[2] * qsi[2]);
-        qg[1] = Sm * qsi[1] / Fm;
-        qg[2] = Sm * qsi[2] / Fm;
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < NV; ++i) qg[i] = qfv[i];
     }
-    // assemble_sol (src/solver_2d.f90:1339-1626)
-    double* qc = qg;
     const long long cell = (long long)k * nx + j;
     bool anynan = false;
 #pragma unroll
@@ -1085,6 +1356,7 @@ __global__ void __launch_bounds__(128, IMEX_STAGE2_MINB)
           if (qc[4 + i] > -1.0e-7) qc[4 + i] = 0.0;
       }
     }
+    double qpv[NP];
     qc_to_qp<NS>(P, qc, qpv);
     if (qpv[3] < 273.0) record_error(clk, 4, cell);
     double ssum = 0.0;
@@ -1106,20 +1378,7 @@ __global__ void __launch_bounds__(128, IMEX_STAGE2_MINB)
       for (int i = 0; i < NV; ++i) qc[i] = 0.0;
     }
 #pragma unroll
-    for (int i = 0; i < NV; ++i) q[c + (size_t)i * P.plane] = qc[i];
-  }
-  // counters
-  for (int off = 16; off > 0; off >>= 1) {
-    newton_cells += __shfl_down_sync(0xffffffffu, newton_cells, off);
-    newton_iters += __shfl_down_sync(0xffffffffu, newton_iters, off);
-    trials += __shfl_down_sync(0xffffffffu, trials, off);
-    maxit += __shfl_down_sync(0xffffffffu, maxit, off);
-  }
-  if ((threadIdx.x & 31) == 0 && newton_cells) {
-    atomicAdd(&clk->newton_cells, (unsigned long long)newton_cells);
-    atomicAdd(&clk->newton_iters, (unsigned long long)newton_iters);
-    atomicAdd(&clk->lnsrch_trials, (unsigned long long)trials);
-    atomicAdd(&clk->newton_maxit, (unsigned long long)maxit);
+    for (int i = 0; i < NV; ++i) q[c + i * N] = qc[i];
   }
 }
 
@@ -1189,6 +1448,11 @@ __global__ void k_step_begin(DevClock* clk, double max_dt, int reset_cells) {
   clk->lnsrch_trials = 0;
   clk->newton_maxit = 0;
   for (int b = 0; b < 16; ++b) clk->hist[b] = 0;
+}
+
+// Empties the stage-2 Newton lists (before each stage 2).
+__global__ void k_nw_reset(DevClock* clk) {
+  for (int i = 0; i < 4; ++i) clk->nw_count[i] = 0;
 }
 
 // dt from the CFL minimum with the driver's clipping (src/IMEX_SfloW2D.f90:359-381).
