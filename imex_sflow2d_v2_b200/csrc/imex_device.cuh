@@ -29,6 +29,12 @@
 #ifndef IMEX_NOINL
 #define IMEX_NOINL __device__ __noinline__
 #endif
+// Functions with one or two call sites per kernel (the Newton pieces, the
+// mass-exchange terms) are inlined: their per-cell arrays then live in
+// registers instead of being passed through the stack.
+#ifndef IMEX_FLAT
+#define IMEX_FLAT __device__ __forceinline__
+#endif
 
 namespace imex {
 
@@ -646,7 +652,7 @@ struct CPrefix {
 };
 
 template <int NS>
-IMEX_NOINL void implicit_prefix_c(const DevParams& P, const cplx* q, CPrefix<NS>& pre) {
+IMEX_FLAT void implicit_prefix_c(const DevParams& P, const cplx* q, CPrefix<NS>& pre) {
   if (!P.rheology_flag || !(q[0].re > EPS)) return;
   cplx inv = rdiv(1.0, q[0]);
   cplx xs[NS];
@@ -671,7 +677,7 @@ IMEX_NOINL void implicit_prefix_c(const DevParams& P, const cplx* q, CPrefix<NS>
 }
 
 template <int NS>
-IMEX_NOINL void implicit_terms_c(const DevParams& P, double bx, double by, const cplx* q,
+IMEX_FLAT void implicit_terms_c(const DevParams& P, double bx, double by, const cplx* q,
                                  const CPrefix<NS>& pre, cplx& nh2, cplx& nh3) {
   nh2 = C(0.0, 0.0);
   nh3 = C(0.0, 0.0);

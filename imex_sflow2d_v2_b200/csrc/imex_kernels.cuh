@@ -151,7 +151,7 @@ struct Tile {
 // `stage` selects the RK-stage arrays' view of never-solved inlet-interior
 // neighbours (all zero) instead of the module qp view (zero with T_ambient).
 template <int NS>
-__device__ __noinline__ void cell_faces(const DevParams& P, const Tile<NS>& T, int lx, int ly, int j, int k,
+IMEX_FLAT void cell_faces(const DevParams& P, const Tile<NS>& T, int lx, int ly, int j, int k,
                            int dir, bool stage, double time, const RingCell* ring,
                            double* Fm, double* Fp) {
   constexpr int NV = 4 + NS, NP = 6 + NS;
@@ -289,7 +289,7 @@ __device__ __noinline__ void cell_faces(const DevParams& P, const Tile<NS>& T, i
 // One interface: left/lower state from cell a, right/upper from cell b.
 // Writes the KT flux H (n_vars) and max(|a+|,|a-|) for the CFL.
 template <int NS>
-__device__ void interface_flux(const DevParams& P, const Tile<NS>& T, int dir, int la_x,
+IMEX_FLAT void interface_flux(const DevParams& P, const Tile<NS>& T, int dir, int la_x,
                                int la_y, int ja, int ka, bool a_in, bool b_in, double gcf,
                                bool stage, double time, const RingCell* ring, double* H,
                                double& amax_flux, double& aneg_out, double& apos_out) {
@@ -303,24 +303,28 @@ __device__ void interface_flux(const DevParams& P, const Tile<NS>& T, int dir, i
   const bool b_int = rad && b_in && (ib & CI_SRC_MASK) == 1;
   const uint8_t flag_b_m = (dir == 1) ? CI_W : CI_S;  // b's inlet lies on its minus side
   const uint8_t flag_a_p = (dir == 1) ? CI_E : CI_N;
+  // reconstruction of the sides that need it, through one call site
+  const bool comp_a = a_in && (!b_in || !a_int);
+  const bool comp_b = b_in && (!a_in || !b_int);
+#pragma unroll 1
+  for (int side = 0; side < 2; ++side) {
+    if (!(side == 0 ? comp_a : comp_b)) continue;
+    cell_faces<NS>(P, T, side ? lb_x : la_x, side ? lb_y : la_y, side ? jb : ja, side ? kb : ka,
+                   dir, stage, time, ring, tmpm, tmpp);
+#pragma unroll
+    for (int i = 0; i < NP; ++i) {
+      if (side == 0) QL[i] = tmpp[i];   // a's plus face
+      else QR[i] = tmpm[i];             // b's minus face
+    }
+  }
   if (!a_in) {  // domain boundary on the minus side: both states from b's minus face
-    cell_faces<NS>(P, T, lb_x, lb_y, jb, kb, dir, stage, time, ring, QR, tmpp);
 #pragma unroll
     for (int i = 0; i < NP; ++i) QL[i] = QR[i];
   } else if (!b_in) {
-    cell_faces<NS>(P, T, la_x, la_y, ja, ka, dir, stage, time, ring, tmpm, QL);
 #pragma unroll
     for (int i = 0; i < NP; ++i) QR[i] = QL[i];
   } else {
-    bool have_a = false, have_b = false;
-    if (!a_int) {
-      cell_faces<NS>(P, T, la_x, la_y, ja, ka, dir, stage, time, ring, tmpm, QL);
-      have_a = true;
-    }
-    if (!b_int) {
-      cell_faces<NS>(P, T, lb_x, lb_y, jb, kb, dir, stage, time, ring, QR, tmpp);
-      have_b = true;
-    }
+    const bool have_a = comp_a, have_b = comp_b;
     if (a_int) {
       // never solved: only the ring copy of src/solver_2d.f90:3768-3771 fills it
       bool copy = have_b && (ib & flag_b_m) && (ib & CI_SRC_MASK) == 2 &&
@@ -456,82 +460,75 @@ __global__ void __launch_bounds__(FLUX_THREADS, IMEX_FLUX_MINB)
     S.tile.info[ly][lx] = inf;
   }
   __syncthreads();
-  // interfaces
+  // interfaces: x faces (e < NXI) then y faces, one interface per thread
   const RingCell* rg = ring;
   for (int e = threadIdx.x; e < NXI + NYI; e += blockDim.x) {
-    int dir, ia_x, ia_y, ja, ka;
-    bool a_in, b_in;
-    double gcf;
-    if (e < NXI) {
-      dir = 1;
-      int jj = e % (TX + 1), kk = e / (TX + 1);
+    const int dir = (e < NXI) ? 1 : 2;
+    int jj, kk, ja, ka, ia_x, ia_y;
+    bool a_in, b_in, sa, sb_;
+    if (dir == 1) {
       // interface between cells (j0+jj-1) and (j0+jj) in row k0+kk
+      jj = e % (TX + 1);
+      kk = e / (TX + 1);
       ja = j0 + jj - 1;
       ka = k0 + kk;
       ia_x = jj - 1 + HALO;
       ia_y = kk + HALO;
-      if (ka >= ny || ja + 1 > nx) { S.ax[kk][jj] = 0.0; continue; }
-      a_in = ja >= 0;
-      b_in = ja + 1 < nx;
-      bool sa = a_in && (S.tile.info[ia_y][ia_x] & 128);
-      bool sb_ = b_in && (S.tile.info[ia_y][ia_x + 1] & 128);
-      if (!(sa || sb_)) { S.ax[kk][jj] = 0.0; continue; }
-      gcf = P.slope_correction_flag ? gcsx[(size_t)ka * (nx + 1) + (ja + 1)] : 1.0;
-      double H[NV], amax, aN, aP;
-      interface_flux<NS>(P, S.tile, 1, ia_x, ia_y, ja, ka, a_in, b_in, gcf, true, time, rg, H,
-                         amax, aN, aP);
-      // CFL from the timestep view when an inlet-interior cell is in the stencil
-      bool dual = false;
-      if (P.radial_source_flag) {
-        for (int d = -1; d <= 2; ++d) {
-          int cx = ia_x + d;
-          int cj = ja + d;
-          if (cj >= 0 && cj < nx && (S.tile.info[ia_y][cx] & CI_SRC_MASK) == 1) dual = true;
-        }
-      }
-      if (dual) {
-        double H2[NV];
-        interface_flux<NS>(P, S.tile, 1, ia_x, ia_y, ja, ka, a_in, b_in, gcf, false, time, rg,
-                           H2, amax, aN, aP);
-      }
-#pragma unroll
-      for (int i = 0; i < NV; ++i) S.Hx[i][kk][jj] = H[i];
-      S.ax[kk][jj] = amax;
     } else {
-      dir = 2;
-      int e2 = e - NXI;
-      int jj = e2 % TX, kk = e2 / TX;
+      const int e2 = e - NXI;
+      jj = e2 % TX;
+      kk = e2 / TX;
       ja = j0 + jj;
       ka = k0 + kk - 1;
       ia_x = jj + HALO;
       ia_y = kk - 1 + HALO;
-      if (ja >= nx || ka + 1 > ny) { S.ay[kk][jj] = 0.0; continue; }
+    }
+    double& a_slot = (dir == 1) ? S.ax[kk][jj] : S.ay[kk][jj];
+    const bool exists = (dir == 1) ? !(ka >= ny || ja + 1 > nx) : !(ja >= nx || ka + 1 > ny);
+    if (!exists) { a_slot = 0.0; continue; }
+    if (dir == 1) {
+      a_in = ja >= 0;
+      b_in = ja + 1 < nx;
+      sa = a_in && (S.tile.info[ia_y][ia_x] & 128);
+      sb_ = b_in && (S.tile.info[ia_y][ia_x + 1] & 128);
+    } else {
       a_in = ka >= 0;
       b_in = ka + 1 < ny;
-      bool sa = a_in && (S.tile.info[ia_y][ia_x] & 128);
-      bool sb_ = b_in && (S.tile.info[ia_y + 1][ia_x] & 128);
-      if (!(sa || sb_)) { S.ay[kk][jj] = 0.0; continue; }
-      gcf = P.slope_correction_flag ? gcsy[(size_t)(ka + 1) * nx + ja] : 1.0;
-      double H[NV], amax, aN, aP;
-      interface_flux<NS>(P, S.tile, 2, ia_x, ia_y, ja, ka, a_in, b_in, gcf, true, time, rg, H,
-                         amax, aN, aP);
-      bool dual = false;
-      if (P.radial_source_flag) {
-        for (int d = -1; d <= 2; ++d) {
-          int cy = ia_y + d;
-          int ck = ka + d;
-          if (ck >= 0 && ck < ny && (S.tile.info[cy][ia_x] & CI_SRC_MASK) == 1) dual = true;
-        }
+      sa = a_in && (S.tile.info[ia_y][ia_x] & 128);
+      sb_ = b_in && (S.tile.info[ia_y + 1][ia_x] & 128);
+    }
+    if (!(sa || sb_)) { a_slot = 0.0; continue; }
+    double gcf = 1.0;
+    if (P.slope_correction_flag)
+      gcf = (dir == 1) ? gcsx[(size_t)ka * (nx + 1) + (ja + 1)] : gcsy[(size_t)(ka + 1) * nx + ja];
+    // CFL from the timestep view when an inlet-interior cell is in the stencil
+    bool dual = false;
+    if (P.radial_source_flag) {
+      for (int d = -1; d <= 2; ++d) {
+        const int cx = (dir == 1) ? ia_x + d : ia_x, cy = (dir == 1) ? ia_y : ia_y + d;
+        const int cg = (dir == 1) ? ja + d : ka + d, cn = (dir == 1) ? nx : ny;
+        if (cg >= 0 && cg < cn && (S.tile.info[cy][cx] & CI_SRC_MASK) == 1) dual = true;
       }
-      if (dual) {
-        double H2[NV];
-        interface_flux<NS>(P, S.tile, 2, ia_x, ia_y, ja, ka, a_in, b_in, gcf, false, time, rg,
-                           H2, amax, aN, aP);
+    }
+    double H[NV], amax = 0.0, aN, aP;
+#pragma unroll 1
+    for (int pass = 0; pass < (dual ? 2 : 1); ++pass) {
+      double Hp[NV];
+      interface_flux<NS>(P, S.tile, dir, ia_x, ia_y, ja, ka, a_in, b_in, gcf, pass == 0, time, rg,
+                         Hp, amax, aN, aP);
+      if (pass == 0) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) H[i] = Hp[i];
       }
+    }
+    if (dir == 1) {
+#pragma unroll
+      for (int i = 0; i < NV; ++i) S.Hx[i][kk][jj] = H[i];
+    } else {
 #pragma unroll
       for (int i = 0; i < NV; ++i) S.Hy[i][kk][jj] = H[i];
-      S.ay[kk][jj] = amax;
     }
+    a_slot = amax;
   }
   __syncthreads();
   // cells: divergence, explicit terms, CFL
@@ -595,7 +592,7 @@ constexpr int NEWTON_MAX_IT = 100;
 constexpr double NEWTON_TOLF = 1.0e-10, NEWTON_STPMX = 100.0;
 
 template <int NS>
-__device__ __noinline__ void eval_f(const DevParams& P, const double* qj, const double* qj_old,
+IMEX_FLAT void eval_f(const DevParams& P, const double* qj, const double* qj_old,
                        const double* Rj, double bx, double by, double dt, double* f,
                        double& scal_f) {
   constexpr int NV = 4 + NS;
@@ -618,7 +615,7 @@ __device__ __noinline__ void eval_f(const DevParams& P, const double* qj, const 
 // Newton direction: explicit rows diagonal, 2x2 Cramer on rows/cols 2,3
 // (src/solver_2d.f90:1879-1901).
 template <int NS>
-__device__ __noinline__ void newton_direction(const DevParams& P, double bx, double by, double dt,
+IMEX_FLAT void newton_direction(const DevParams& P, double bx, double by, double dt,
                                               const double* qj_org, const double* qj_rel,
                                               const double* rt, double* dd, double* J2,
                                               double* J3) {
@@ -637,13 +634,14 @@ __device__ __noinline__ void newton_direction(const DevParams& P, double bx, dou
     for (int m = 0; m < NV; ++m) qc[m] = mulr(C(qj_rel[m], (m == col) ? P.hstep : 0.0), qj_org[m]);
     cplx nh2, nh3;
     implicit_terms_c<NS>(P, bx, by, qc, pre, nh2, nh3);
-    double* Lc = (col == 1) ? J2 : J3;
 #pragma unroll
     for (int r = 0; r < NV; ++r) {
       double nim = (r == 1) ? nh2.im : ((r == 2) ? nh3.im : 0.0);
       double jac = 1.0 * nim * P.one_by_h;
-      double l0 = (r == col) ? 1.0 * qj_org[col] : 0.0;
-      Lc[r] = l0 - dt * 1.0 * jac;
+      double l0 = (r == col) ? 1.0 * (col == 1 ? qj_org[1] : qj_org[2]) : 0.0;
+      double v = l0 - dt * 1.0 * jac;
+      if (col == 1) J2[r] = v;
+      else J3[r] = v;
     }
   }
   double d1[NV];
@@ -739,7 +737,7 @@ __device__ bool newton_iter1(const DevParams& P, double* qj, const double* qj_ol
 // cubic model's value is clamped to <= alam/2 and then maxed with alam/2.
 // The trials are capped at 4096; the cap exits like alam < alamin.
 template <int NS>
-__device__ __noinline__ bool newton_iterk(const DevParams& P, double* qj, const double* qj_old,
+IMEX_FLAT bool newton_iterk(const DevParams& P, double* qj, const double* qj_old,
                                           const double* Rj, double bx, double by, double dt,
                                           const double* qj_org, double* qj_rel, double* rt,
                                           double& scal_f, long long& trials) {
@@ -838,7 +836,7 @@ __device__ __noinline__ bool newton_iterk(const DevParams& P, double* qj, const 
 
 // ============================================================ mass exchange
 template <int NS>
-__device__ __noinline__ void mass_exchange(const DevParams& P, const double* qpj, double bx, double by,
+IMEX_FLAT void mass_exchange(const DevParams& P, const double* qpj, double bx, double by,
                               const double* erod, double dtl, double* ers, double* dep,
                               double& cpe, double& cpl, double* eqns, double& topo,
                               bool& dep_neg) {
