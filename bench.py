@@ -61,16 +61,34 @@ def workload(n, layer):
     return configs.fractal_inlet(n=n, initial_layer=layer)
 
 
-def bytes_per_cell(ns, erosion):
-    """Algorithmic bytes per cell and launch of each kernel (8-byte values)."""
+def bytes_per_cell(ns, erosion, listed=(1.0, 0.0, 0.0)):
+    """Algorithmic bytes per grid cell and step of each timed kernel group
+    (8-byte values, 1-byte masks, 4-byte list entries).  `listed` is the
+    fraction of cells that run Newton iteration 2, 3 and 4.. (each such pass
+    reads and writes the cell's Newton state)."""
     nv = 4 + ns
-    mask = 8 + 1                                   # q1 read, mask byte written
-    flux = 8 * nv + 1 + 16 + 8 * nv                # q, mask, B'x, B'y read; X written
-    stage2 = 8 * nv + 8 * nv + 1 + 16 + 8 * nv     # q, X, mask, B' read; q written
-    out = {"mask": mask, "flux": flux, "stage2": stage2}
-    if erosion:                                    # q, mask, B' read; q written;
+    out = {
+        "mask": 8 + 1,                                  # q1 read, mask byte written
+        "flux": 8 * nv + 1 + 16 + 8 * nv,               # q, mask, B'x, B'y read; X written
+        # q, X, mask, B' read; q_si, Rj, iterate, residual, |r|^2, status, list written
+        "stage2_first": 16 * nv + 17 + 32 * nv + 8 + 1 + 4,
+        # per pass and listed cell: q, Rj, q_si, iterate, residual, |r|^2, B', list
+        # read; iterate, residual, |r|^2, list written
+        "stage2_iter": sum(listed) * (40 * nv + 8 + 16 + 4 + 16 * nv + 8 + 4),
+        "stage2_post": 8 * nv + 1 + 16 + 1 + 8 * nv,    # iterate, status, q_si(2), mask; q
+    }
+    if erosion:                                         # q, mask, B' read; q written;
         out["erosion"] = 8 * nv + 1 + 16 + 8 * nv + 2 * 3 * 8 * ns  # 3 planes per class r+w
     return out
+
+
+def fp64_counts():
+    """FP64 instructions (DADD+DMUL+DFMA, per thread) per cell of each kernel
+    group, from the ncu capture summarised in profiles/fp64_inst_per_cell.json."""
+    try:
+        return json.load(open(os.path.join(ROOT, "profiles", "fp64_inst_per_cell.json")))
+    except Exception:
+        return {}
 
 
 class ClockSampler:
@@ -237,10 +255,15 @@ def main():
 
     # roofline of the dominant kernel (event times from the timed region)
     erosion = bool(p.erosion_coeff != 0.0 or p.settling_flag)
-    bpc = bytes_per_cell(p.n_solid, erosion)
-    dom = max(kt, key=lambda k: kt[k][0])
-    dom_ms, dom_n = kt[dom]
-    avg_s = dom_ms / max(dom_n, 1) * 1e-3
+    hist = list(s1.newton_hist)
+    ncells_newton = max(1, s1.newton_cells)
+    listed = (sum(hist[1:]) / cells, sum(hist[2:]) / cells, sum(hist[3:]) / cells)
+    bpc = bytes_per_cell(p.n_solid, erosion, listed)
+    timed = {k: v for k, v in kt.items() if v[1] > 0}
+    dom = max(timed, key=lambda k: timed[k][0])
+    steps_timed = args.steps
+    dom_ms = timed[dom][0] / steps_timed            # per step (a group may be several launches)
+    avg_s = dom_ms * 1e-3
     alg_bytes = bpc[dom] * cells
     peak = None
     peak_src = "fallback"
@@ -261,6 +284,16 @@ def main():
         fp64_peak = measure_fp64_peak(local)
     except Exception:
         pass
+    # FP64 pipe: instructions per cell (ncu) x cells / live kernel time, against
+    # the measured FMA-chain peak (one FP64 instruction per lane per FMA)
+    fpc = fp64_counts()
+    fp64 = None
+    if fp64_peak and dom in fpc:
+        inst_s = fpc[dom] * cells / avg_s
+        peak_inst_s = fp64_peak * 1e9 / 2.0
+        fp64 = {"kernel": dom, "inst_per_cell": fpc[dom], "achieved_inst_per_s": inst_s,
+                "peak_inst_per_s": peak_inst_s, "frac": inst_s / peak_inst_s,
+                "peak_source": "measured FP64 FMA chain (k_fp64_probe)"}
 
     # end to end through the public API with pinned host buffers
     e2e = None
@@ -303,14 +336,16 @@ def main():
                        "solve_cells_per_step": int(s1.solve_cells)},
             "newton_iters_per_cell": newton_per_cell,
             "newton_cells_per_step": s1.newton_cells,
+            "newton_hist": hist[:6],
+            "lnsrch_trials_per_cell": s1.lnsrch_trials / ncells_newton,
             "gpu_launches": launches,
             "clocks": clocks,
             "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
                          "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
                          "avg_launch_ms": avg_s * 1e3,
-                         "kernel_ms": {k: v[0] / max(v[1], 1) for k, v in kt.items()},
-                         "fp64_fma_peak_gflops": fp64_peak},
+                         "kernel_ms_per_step": {k: v[0] / steps_timed for k, v in timed.items()},
+                         "fp64_pipe": fp64, "fp64_fma_peak_gflops": fp64_peak},
             "e2e": e2e,
             "cpu_baseline": cb,
             "errors": int(s1.error_mask),

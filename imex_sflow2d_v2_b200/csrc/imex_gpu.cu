@@ -96,6 +96,45 @@ int grid_1d(long long n, int threads) {
   return (int)std::min<long long>(std::max<long long>(b, 1), 148LL * 64);
 }
 
+// Kernel ids for imex_gpu_kernel_times.
+enum {
+  KID_MASK = 0,
+  KID_FLUX = 1,
+  KID_S2_FIRST = 2,   // stage 2 up to Newton iteration 1
+  KID_S2_ITER = 3,    // Newton iterations 2.. (both list passes and the tail)
+  KID_S2_POST = 4,    // sign guard and assembly
+  KID_EROSION = 5,
+  KID_N = 6
+};
+
+cudaEvent_t pool_event(ImexCtx* ctx) {
+  if (ctx->ev_used == ctx->ev_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    ctx->ev_pool.push_back(e);
+  }
+  return ctx->ev_pool[ctx->ev_used++];
+}
+
+struct ProfScope {
+  ImexCtx* ctx;
+  int kid;
+  cudaEvent_t a = nullptr, b = nullptr;
+  ProfScope(ImexCtx* c, int k) : ctx(c), kid(k) {
+    if (ctx->prof) {
+      a = pool_event(ctx);
+      b = pool_event(ctx);
+      cudaEventRecord(a, ctx->stream);
+    }
+  }
+  ~ProfScope() {
+    if (ctx->prof) {
+      cudaEventRecord(b, ctx->stream);
+      ctx->ev_pending.push_back({kid, {a, b}});
+    }
+  }
+};
+
 // ------------------------------------------------------- launch helpers
 template <int NS>
 cudaError_t launch_flux_ns(ImexCtx* ctx) {
@@ -131,17 +170,26 @@ cudaError_t launch_stage2_ns(ImexCtx* ctx) {
   // list passes: one resident wave (IMEX_STAGE2_MINB blocks per SM), grid-stride
   const int lgrid = std::min(grid, 148 * IMEX_STAGE2_MINB);
   k_nw_reset<<<1, 1, 0, ctx->stream>>>(ctx->clk);
-  k_stage2_first<NS><<<grid, STAGE2_THREADS, 0, ctx->stream>>>(
-      ctx->dP, ctx->q, ctx->X, ctx->mask, ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy, ctx->Byy, ctx->gc,
-      ctx->nw, ctx->clk);
-  k_stage2_iter<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->Bx, ctx->By,
-                                                               ctx->nw, ctx->clk, 2);
-  k_stage2_iter<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->Bx, ctx->By,
-                                                               ctx->nw, ctx->clk, 3);
-  k_stage2_tail<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->Bx, ctx->By,
-                                                               ctx->nw, ctx->clk);
-  k_stage2_post<NS><<<grid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->mask,
-                                                              ctx->cellinfo, ctx->nw, ctx->clk);
+  {
+    ProfScope ps(ctx, KID_S2_FIRST);
+    k_stage2_first<NS><<<grid, STAGE2_THREADS, 0, ctx->stream>>>(
+        ctx->dP, ctx->q, ctx->X, ctx->mask, ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy, ctx->Byy,
+        ctx->gc, ctx->nw, ctx->clk);
+  }
+  {
+    ProfScope ps(ctx, KID_S2_ITER);
+    k_stage2_iter<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->Bx,
+                                                                 ctx->By, ctx->nw, ctx->clk, 2);
+    k_stage2_iter<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->Bx,
+                                                                 ctx->By, ctx->nw, ctx->clk, 3);
+    k_stage2_tail<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->Bx,
+                                                                 ctx->By, ctx->nw, ctx->clk);
+  }
+  {
+    ProfScope ps(ctx, KID_S2_POST);
+    k_stage2_post<NS><<<grid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->mask,
+                                                                ctx->cellinfo, ctx->nw, ctx->clk);
+  }
   ctx->launches += 6;
   return cudaGetLastError();
 }
@@ -188,37 +236,6 @@ bool erosion_active(const ImexCtx* ctx) {
   return p.erosion_coeff != 0.0 || p.settling_flag || p.entrainment_flag;
 }
 
-// Kernel ids for imex_gpu_kernel_times.
-enum { KID_MASK = 0, KID_FLUX = 1, KID_STAGE2 = 2, KID_EROSION = 3, KID_N = 4 };
-
-cudaEvent_t pool_event(ImexCtx* ctx) {
-  if (ctx->ev_used == ctx->ev_pool.size()) {
-    cudaEvent_t e;
-    cudaEventCreate(&e);
-    ctx->ev_pool.push_back(e);
-  }
-  return ctx->ev_pool[ctx->ev_used++];
-}
-
-struct ProfScope {
-  ImexCtx* ctx;
-  int kid;
-  cudaEvent_t a = nullptr, b = nullptr;
-  ProfScope(ImexCtx* c, int k) : ctx(c), kid(k) {
-    if (ctx->prof) {
-      a = pool_event(ctx);
-      b = pool_event(ctx);
-      cudaEventRecord(a, ctx->stream);
-    }
-  }
-  ~ProfScope() {
-    if (ctx->prof) {
-      cudaEventRecord(b, ctx->stream);
-      ctx->ev_pending.push_back({kid, {a, b}});
-    }
-  }
-};
-
 // Device part of one driver-loop pass: mask, fluxes + CFL, dt clip, stage 2
 // , erosion/deposition, t += dt.
 cudaError_t enqueue_step(ImexCtx* ctx) {
@@ -235,10 +252,7 @@ cudaError_t enqueue_step(ImexCtx* ctx) {
   }
   k_dt_clip<<<1, 1, 0, ctx->stream>>>(ctx->clk, 1);
   ctx->launches += 1;
-  {
-    ProfScope ps(ctx, KID_STAGE2);
-    if ((e = launch_stage2(ctx)) != cudaSuccess) return e;
-  }
+  if ((e = launch_stage2(ctx)) != cudaSuccess) return e;
   if (erosion_active(ctx)) {
     ProfScope ps(ctx, KID_EROSION);
     if ((e = launch_erosion(ctx)) != cudaSuccess) return e;

@@ -220,7 +220,7 @@ class ImexSolver:
         return self._check(self.lib.imex_gpu_set_stream(self._h, C.c_void_p(stream_handle or None)),
                            "set_stream")
 
-    KERNELS = ("mask", "flux", "stage2", "erosion")
+    KERNELS = ("mask", "flux", "stage2_first", "stage2_iter", "stage2_post", "erosion")
 
     def profile(self, enable=True):
         return self._check(self.lib.imex_gpu_profile(self._h, int(bool(enable))), "profile")

@@ -236,12 +236,13 @@ int imex_gpu_set_stream(ImexCtx* ctx, void* stream);
 int imex_gpu_device_state(ImexCtx* ctx, double** q_dev, int64_t* pitch);
 
 /* Measurement helpers (no counterpart in the reference).
- * imex_gpu_profile(ctx, 1) records CUDA events around the mask, flux,
- * stage-2 and erosion/deposition kernels that imex_gpu_advance launches
- * without a graph, on the context stream; imex_gpu_kernel_times returns, per
- * kernel id (0 mask, 1 flux, 2 stage 2, 3 erosion/deposition; n_kernels must
- * be at least 4), the summed event time in ms and the launch count since the
- * last call.  imex_gpu_measure_fp64_peak times an FP64 FMA-chain kernel
+ * imex_gpu_profile(ctx, 1) records CUDA events around the kernels that
+ * imex_gpu_advance launches without a graph, on the context stream;
+ * imex_gpu_kernel_times returns, per kernel id, the summed event time in ms
+ * and the number of timed launches since the last call.  Ids: 0 mask,
+ * 1 flux (stage 1 + CFL), 2 stage 2 up to Newton iteration 1, 3 Newton
+ * iterations 2.. (three launches), 4 stage-2 assembly, 5 erosion/deposition;
+ * n_kernels must be at least 6.  imex_gpu_measure_fp64_peak times an FP64 FMA-chain kernel
  * and returns the achieved GFLOP/s (2 flops per FMA). */
 int imex_gpu_profile(ImexCtx* ctx, int enable);
 int imex_gpu_kernel_times(ImexCtx* ctx, double* total_ms, int64_t* launches, int n_kernels);
