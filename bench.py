@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--ens-members", type=int, default=256)
+    ap.add_argument("--ens-steps", type=int, default=1000)
+    ap.add_argument("--no-ensemble", action="store_true")
     return ap.parse_args()
 
 
@@ -173,6 +176,40 @@ def cpu_baseline(args, threads=None):
             "sample": "%dx%d instance of the same generator (seed, physics, 2 m layer), "
                       "%d steps after 2 untimed, %.1f s, OpenMP %d threads"
                       % (args.cpu_n, args.cpu_n, steps, el, cores, )}
+
+
+def run_ensemble(args):
+    """Batched ensemble (fourth workload): members/hour for `ens_steps` steps
+    of every member, one CUDA graph per step over all members."""
+    from imex_sflow2d_v2_b200 import configs
+    from imex_sflow2d_v2_b200.solver import ImexEnsemble
+    mem = configs.ensemble_members(n_members=args.ens_members)
+    ens = ImexEnsemble([(p, st) for p, st, q, s in mem])
+    for m, (p, st, q, s) in enumerate(mem):
+        ens.member(m).set_state(q, 0.0)
+        ens.member(m).set_clock(0.0, 1e-2)
+    cells = sum(p.nx * p.ny for p, *_ in mem)
+    t0 = time.perf_counter()
+    rc, bad = ens.advance(args.ens_steps)
+    el = time.perf_counter() - t0
+    k, tried = ens.tuning()
+    flagged = []
+    for m in range(len(mem)):
+        st_ = ens.member(m).stats()
+        if st_.error_mask:
+            flagged.append({"member": m, "error_mask": int(st_.error_mask)})
+    ens.close()
+    return {"members": args.ens_members, "steps_per_member": args.ens_steps,
+            "cells_total": cells, "seconds": el,
+            "members_per_hour": args.ens_members * 3600.0 / el,
+            "cell_updates_per_s": cells * args.ens_steps / el,
+            "k_streams": k, "tuning_ms_per_step": tried,
+            "timing": "host clock around the synchronous advance call (tuning steps included)",
+            "members_with_reference_checks": flagged[:16],
+            "n_members_with_reference_checks": len(flagged),
+            "data": "synthetic (seeded sampler: side U{256..1024}, bump height U[5,50] m, "
+                    "sigma U[50,300] m, mfr logU[1e6,1e8] kg/s, T U[600,1200] K, "
+                    "d logU[1e-5,1e-3] m)"}
 
 
 def run_reference(args, rank, world):
@@ -320,6 +357,10 @@ def main():
                "h2d_bytes_per_step": nv * cells * 8, "d2h_bytes_per_step": nv * cells * 8,
                "steps": args.e2e_steps}
 
+    g.close()
+    ensemble = None
+    if rank == 0 and world == 1 and not args.no_ensemble:
+        ensemble = run_ensemble(args)
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(args)
@@ -349,6 +390,7 @@ def main():
             "e2e": e2e,
             "cpu_baseline": cb,
             "errors": int(s1.error_mask),
+            "ensemble": ensemble,
         }
         print(json.dumps(line), flush=True)
     g.close()

@@ -427,3 +427,32 @@ def fractal_inlet(n=4096, dx=10.0, hurst=0.8, relief=800.0, slope_deg=15.0,
     else:
         q = np.zeros((4 + ns, n, n), order="F")
     return p, static, q
+
+
+def ensemble_members(n_members=256, side_min=256, side_max=1024, dx=2.0, seed=20261204,
+                     bump_h=(5.0, 50.0), bump_sigma=(50.0, 300.0), mfr=(1.0e6, 1.0e8),
+                     T_source=(600.0, 1200.0), diam=(1.0e-5, 1.0e-3), r_source=20.0):
+    """Batched-ensemble workload (fourth workload): members on their own
+    square grids of 2 m cells, side uniform in [side_min, side_max]; a
+    Gaussian bump of uniform random height and sigma; a radial inlet of
+    r = 20 m with log-uniform mass flow, uniform temperature and one solid
+    class of log-uniform diameter (95% solid by mass, Voellmy friction as in
+    the radial-current workload).  The sampling follows the reference's
+    ensemble example (EXAMPLES/EXAMPLE_ENSEMBLE_ETNA/create_ensemble.py:35-55:
+    log-uniform and uniform 1-D sampling).  Returns a list of
+    (params, static, q, sample) with `sample` the drawn values."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_members):
+        side = int(rng.integers(side_min, side_max + 1))
+        s = {"side": side,
+             "bump_h": float(rng.uniform(*bump_h)),
+             "bump_sigma": float(rng.uniform(*bump_sigma)),
+             "mfr": float(10.0 ** rng.uniform(np.log10(mfr[0]), np.log10(mfr[1]))),
+             "T_source": float(rng.uniform(*T_source)),
+             "diam": float(10.0 ** rng.uniform(np.log10(diam[0]), np.log10(diam[1])))}
+        p, st, q = radial_current(nx=side, ny=side, dx=dx, bump_h=s["bump_h"],
+                                  bump_sigma=s["bump_sigma"], r_source=r_source, mfr=s["mfr"],
+                                  T_source=s["T_source"], xs=(0.95,), diam=(s["diam"],))
+        out.append((p, st, q, s))
+    return out

@@ -47,6 +47,7 @@ struct ImexCtx {
   bool exchange = false;         // erosion/deposition planes present
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
+  int64_t graph_launches = 0;    // kernels in one replay of graph_exec
   int64_t launches = 0;
   uint32_t error_mask_acc = 0;
   std::string last_error;
@@ -761,11 +762,12 @@ int imex_gpu_advance(ImexCtx* ctx, int n_steps, int use_graph, double* t) {
       if (e2 != cudaSuccess) return fail(ctx, IMEX_ECUDA, cudaGetErrorString(e2));
       ctx->graph = g;
       CK(cudaGraphInstantiate(&ctx->graph_exec, g, 0));
+      ctx->graph_launches = ctx->launches - l0;
       ctx->launches = l0;
     }
     for (int s = 0; s < n_steps; ++s) {
       CK(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
-      ctx->launches += 6;
+      ctx->launches += ctx->graph_launches;
     }
   } else {
     for (int s = 0; s < n_steps; ++s) {
@@ -915,6 +917,250 @@ int imex_gpu_device_state(ImexCtx* ctx, double** q_dev, int64_t* pitch) {
 
 }  // extern "C"
 
+// ================================================================ ensemble
+// Many independent runs (members) on one GPU, each with its own grid and
+// parameters: one context per member, all members' time steps captured into
+// one CUDA graph and replayed.  The graph forks the members over K streams
+// (members dealt largest first to the least loaded stream); K is chosen by
+// timing the first steps with K = 1, 2, 4, ... (each a real step: members
+// are independent, so the results do not depend on K).
+struct ImexEnsemble {
+  int device = 0;
+  std::vector<ImexCtx*> members;
+  cudaStream_t root = nullptr;
+  std::vector<cudaStream_t> workers;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<int64_t> step_launches;  // per member: kernels in one replayed step
+  int k_streams = 0;                 // chosen concurrency (0: not tuned yet)
+  std::vector<int> tried_k;
+  std::vector<float> tried_ms;
+  std::string last_error;
+};
+
+namespace {
+
+constexpr int ENS_MAX_STREAMS = 32;
+
+int ens_fail(ImexEnsemble* e, int code, const std::string& msg) {
+  if (e) e->last_error = msg;
+  return code;
+}
+
+#define CKE(call)                                                             \
+  do {                                                                        \
+    cudaError_t e_ = (call);                                                  \
+    if (e_ != cudaSuccess) return ens_fail(ens, IMEX_ECUDA, cudaGetErrorString(e_)); \
+  } while (0)
+
+void ens_drop_graph(ImexEnsemble* ens) {
+  if (ens->exec) cudaGraphExecDestroy(ens->exec);
+  if (ens->graph) cudaGraphDestroy(ens->graph);
+  ens->exec = nullptr;
+  ens->graph = nullptr;
+}
+
+// Capture one step of every member, forked over k streams.
+int ens_build_graph(ImexEnsemble* ens, int k) {
+  ens_drop_graph(ens);
+  const int n = (int)ens->members.size();
+  std::vector<int> order(n);
+  for (int m = 0; m < n; ++m) order[m] = m;
+  auto cells = [&](int m) { return (double)ens->members[m]->P.nx * ens->members[m]->P.ny; };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cells(a) > cells(b); });
+  std::vector<std::vector<int>> bucket(k);
+  std::vector<double> load(k, 0.0);
+  for (int m : order) {
+    int best = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    bucket[best].push_back(m);
+    load[best] += cells(m);
+  }
+  std::vector<int64_t> l0(n);
+  for (int m = 0; m < n; ++m) l0[m] = ens->members[m]->launches;
+  CKE(cudaStreamBeginCapture(ens->root, cudaStreamCaptureModeThreadLocal));
+  cudaError_t err = cudaEventRecord(ens->fork, ens->root);
+  for (int w = 0; w < k && err == cudaSuccess; ++w) {
+    err = cudaStreamWaitEvent(ens->workers[w], ens->fork, 0);
+    for (int m : bucket[w]) {
+      if (err != cudaSuccess) break;
+      ImexCtx* c = ens->members[m];
+      cudaStream_t saved = c->stream;
+      c->stream = ens->workers[w];
+      err = enqueue_step(c);
+      c->stream = saved;
+    }
+    if (err == cudaSuccess) err = cudaEventRecord(ens->join[w], ens->workers[w]);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(ens->root, ens->join[w], 0);
+  }
+  cudaGraph_t g = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(ens->root, &g);
+  if (err != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return ens_fail(ens, IMEX_ECUDA, cudaGetErrorString(err));
+  }
+  if (e2 != cudaSuccess) return ens_fail(ens, IMEX_ECUDA, cudaGetErrorString(e2));
+  ens->graph = g;
+  CKE(cudaGraphInstantiate(&ens->exec, g, 0));
+  // the capture counted each member's kernels once; replays count them
+  ens->step_launches.assign(n, 0);
+  for (int m = 0; m < n; ++m) {
+    ens->step_launches[m] = ens->members[m]->launches - l0[m];
+    ens->members[m]->launches = l0[m];
+  }
+  return IMEX_OK;
+}
+
+int ens_replay(ImexEnsemble* ens, float* ms) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (ms) {
+    CKE(cudaEventCreate(&a));
+    CKE(cudaEventCreate(&b));
+    CKE(cudaEventRecord(a, ens->root));
+  }
+  CKE(cudaGraphLaunch(ens->exec, ens->root));
+  for (size_t m = 0; m < ens->members.size(); ++m) ens->members[m]->launches += ens->step_launches[m];
+  if (ms) {
+    CKE(cudaEventRecord(b, ens->root));
+    CKE(cudaEventSynchronize(b));
+    CKE(cudaEventElapsedTime(ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+  return IMEX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int imex_gpu_ensemble_create(int n_members, const ImexParams* const* params,
+                             const ImexStatic* const* statics, int device, ImexEnsemble** out) {
+  if (!out || n_members < 1 || !params || !statics) return IMEX_EINVAL;
+  *out = nullptr;
+  ImexEnsemble* ens = new ImexEnsemble();
+  for (int m = 0; m < n_members; ++m) {
+    ImexCtx* c = nullptr;
+    int r = imex_gpu_create(params[m], statics[m], device, &c);
+    if (r != IMEX_OK) {
+      for (ImexCtx* x : ens->members) imex_gpu_destroy(x);
+      delete ens;
+      return r;
+    }
+    ens->members.push_back(c);
+  }
+  ens->device = ens->members[0]->device;
+  CKE(cudaSetDevice(ens->device));
+  CKE(cudaStreamCreateWithFlags(&ens->root, cudaStreamNonBlocking));
+  const int nw = std::min(n_members, ENS_MAX_STREAMS);
+  ens->workers.resize(nw);
+  ens->join.resize(nw);
+  for (int w = 0; w < nw; ++w) {
+    CKE(cudaStreamCreateWithFlags(&ens->workers[w], cudaStreamNonBlocking));
+    CKE(cudaEventCreateWithFlags(&ens->join[w], cudaEventDisableTiming));
+  }
+  CKE(cudaEventCreateWithFlags(&ens->fork, cudaEventDisableTiming));
+  *out = ens;
+  return IMEX_OK;
+}
+
+int imex_gpu_ensemble_destroy(ImexEnsemble* ens) {
+  if (!ens) return IMEX_EINVAL;
+  cudaSetDevice(ens->device);
+  if (ens->root) cudaStreamSynchronize(ens->root);
+  ens_drop_graph(ens);
+  for (cudaStream_t w : ens->workers) cudaStreamDestroy(w);
+  for (cudaEvent_t e : ens->join) cudaEventDestroy(e);
+  if (ens->fork) cudaEventDestroy(ens->fork);
+  if (ens->root) cudaStreamDestroy(ens->root);
+  for (ImexCtx* c : ens->members) imex_gpu_destroy(c);
+  delete ens;
+  return IMEX_OK;
+}
+
+int imex_gpu_ensemble_member(ImexEnsemble* ens, int m, ImexCtx** ctx) {
+  if (!ens || !ctx || m < 0 || m >= (int)ens->members.size()) return IMEX_EINVAL;
+  *ctx = ens->members[m];
+  return IMEX_OK;
+}
+
+int imex_gpu_ensemble_advance(ImexEnsemble* ens, int n_steps, int* first_bad_member) {
+  if (!ens || n_steps < 0) return IMEX_EINVAL;
+  CKE(cudaSetDevice(ens->device));
+  if (first_bad_member) *first_bad_member = -1;
+  // members' own work (set_state, set_clock) is ordered before the graph
+  for (ImexCtx* c : ens->members) CKE(cudaStreamSynchronize(c->stream));
+  const int nmem = (int)ens->members.size();
+  int done = 0;
+  // tuning: one real step per candidate stream count
+  while (ens->k_streams == 0 && done < n_steps) {
+    int k = ens->tried_k.empty() ? 1 : ens->tried_k.back() * 2;
+    if (k > std::min(nmem, ENS_MAX_STREAMS)) {
+      size_t best = 0;
+      for (size_t i = 1; i < ens->tried_ms.size(); ++i)
+        if (ens->tried_ms[i] < ens->tried_ms[best]) best = i;
+      ens->k_streams = ens->tried_k[best];
+      break;
+    }
+    int r = ens_build_graph(ens, k);
+    if (r) return r;
+    float ms = 0.0f;
+    r = ens_replay(ens, &ms);
+    if (r) return r;
+    ens->tried_k.push_back(k);
+    ens->tried_ms.push_back(ms);
+    ++done;
+  }
+  if (done < n_steps) {
+    if (!ens->exec || ens->tried_k.empty() || ens->tried_k.back() != ens->k_streams) {
+      int r = ens_build_graph(ens, ens->k_streams);
+      if (r) return r;
+      ens->tried_k.push_back(ens->k_streams);
+      ens->tried_ms.push_back(-1.0f);
+    }
+    for (; done < n_steps; ++done) {
+      int r = ens_replay(ens, nullptr);
+      if (r) return r;
+    }
+  }
+  CKE(cudaStreamSynchronize(ens->root));
+  int first = IMEX_OK;
+  for (int m = 0; m < nmem; ++m) {
+    ImexCtx* c = ens->members[m];
+    c->x_valid = false;
+    int r = collect_errors(c);
+    if (r != IMEX_OK && first == IMEX_OK) {
+      first = r;
+      if (first_bad_member) *first_bad_member = m;
+    }
+  }
+  return first;
+}
+
+int imex_gpu_ensemble_tuning(ImexEnsemble* ens, int* k_streams, int* n_tried, int* tried_k,
+                             float* tried_ms, int cap) {
+  if (!ens) return IMEX_EINVAL;
+  if (k_streams) *k_streams = ens->k_streams;
+  int n = 0;
+  for (size_t i = 0; i < ens->tried_k.size(); ++i) {
+    if (ens->tried_ms[i] < 0.0f) continue;
+    if (n < cap) {
+      if (tried_k) tried_k[n] = ens->tried_k[i];
+      if (tried_ms) tried_ms[n] = ens->tried_ms[i];
+    }
+    ++n;
+  }
+  if (n_tried) *n_tried = n;
+  return IMEX_OK;
+}
+
+const char* imex_gpu_ensemble_last_error(ImexEnsemble* ens) {
+  return ens ? ens->last_error.c_str() : "null ensemble";
+}
+
+}  // extern "C"
+
 // ======================================================= allocation-free dt
 // imex_gpu_timestep_noalloc: the CFL time step of imex_gpu_timestep for
 // callers that may not allocate device memory when they call it, e.g. a
@@ -1044,7 +1290,7 @@ __global__ void __launch_bounds__(FLUX_THREADS)
 }
 
 // One block folds the tile minima into slot n_tiles of the same array with
-// the rule of the atomic minimum in k_flux (only 0 < m < max_dt lowers dt).
+// the rule of the atomic minimum in k_flux (only 0 <= m < max_dt lowers dt).
 __global__ void __launch_bounds__(1024) k_cfl_fold(const DevParams* __restrict__ Pp,
                                                    double* tile_min, long long n_tiles) {
   __shared__ double red[32];
@@ -1052,7 +1298,7 @@ __global__ void __launch_bounds__(1024) k_cfl_fold(const DevParams* __restrict__
   double m = max_dt;
   for (long long i = threadIdx.x; i < n_tiles; i += blockDim.x) {
     double v = tile_min[i];
-    if (v > 0.0 && v < max_dt) m = fmin_f(m, v);
+    if (v >= 0.0 && v < max_dt) m = fmin_f(m, v);
   }
   for (int off = 16; off > 0; off >>= 1) m = fmin_f(m, __shfl_down_sync(0xffffffffu, m, off));
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;

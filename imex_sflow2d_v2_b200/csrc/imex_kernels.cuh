@@ -575,7 +575,10 @@ __global__ void __launch_bounds__(FLUX_THREADS, IMEX_FLUX_MINB)
   if (threadIdx.x == 0) {
     double m = S.dtmin[0];
     for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmin_f(m, S.dtmin[w]);
-    if (m > 0.0 && m < P.max_dt)
+    // a speed of +inf gives a cell dt of +0.0, which the reference's MIN
+    // keeps; the block minimum is never negative and NaN is filtered by
+    // fmin_f, so the ordered-bits atomicMin sees only non-negative doubles
+    if (m >= 0.0 && m < P.max_dt)
       atomicMin(&clk->dtmin_bits, (unsigned long long)__double_as_longlong(m));
   }
 }
@@ -732,16 +735,32 @@ __device__ bool newton_iter1(const DevParams& P, double* qj, const double* qj_ol
   return newton_converged<NS>(rt, qj_rel, x_old);
 }
 
-// Iterations 2..100: Newton direction and lnsrch (src/solver_2d.f90:
-// 1929-1962, 2019-2224).  Every backtrack after the first halves alam: the
-// cubic model's value is clamped to <= alam/2 and then maxed with alam/2.
-// The trials are capped at 4096; the cap exits like alam < alamin.
+// Iterations 2..100: residual at the iterate, Newton direction and lnsrch
+// (src/solver_2d.f90:1815-1824, 1929-1962, 2019-2224).  The reference
+// evaluates the residual at the start of every iteration; it equals the one
+// left by the previous iteration unless that iteration's line search put the
+// old iterate back (alam < alamin or the trial cap), leaving the residual of
+// its last trial: `stale` marks that case and the residual is evaluated
+// again (the loop only continues after such a restore when the relative
+// step is NaN).  Every backtrack after the first halves alam: the cubic
+// model's value is clamped to <= alam/2 and then maxed with alam/2.  The
+// trials are capped at 4096; the cap exits like alam < alamin.
 template <int NS>
 IMEX_FLAT bool newton_iterk(const DevParams& P, double* qj, const double* qj_old,
                                           const double* Rj, double bx, double by, double dt,
                                           const double* qj_org, double* qj_rel, double* rt,
-                                          double& scal_f, long long& trials) {
+                                          double& scal_f, long long& trials, bool& stale) {
   constexpr int NV = 4 + NS;
+  if (stale) {
+    stale = false;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) qj[i] = qj_rel[i] * qj_org[i];
+    eval_f<NS>(P, qj, qj_old, Rj, bx, by, dt, rt, scal_f);
+    double mx = fabs(rt[0]);
+#pragma unroll
+    for (int i = 1; i < NV; ++i) mx = fmax_f(mx, fabs(rt[i]));
+    if (mx < NEWTON_TOLF) return true;
+  }
   double dd[NV], J2[NV], J3[NV], x_old[NV];
   newton_direction<NS>(P, bx, by, dt, qj_org, qj_rel, rt, dd, J2, J3);
 #pragma unroll
@@ -814,6 +833,7 @@ IMEX_FLAT bool newton_iterk(const DevParams& P, double* qj, const double* qj_old
 #pragma unroll
         for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i];
         scal_f = scal_f_old;
+        stale = true;
         break;
       }
       if (alam == 1.0) {
@@ -827,6 +847,7 @@ IMEX_FLAT bool newton_iterk(const DevParams& P, double* qj, const double* qj_old
 #pragma unroll
       for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i];
       scal_f = scal_f_old;
+      stale = true;
     }
   }
 #pragma unroll
@@ -1020,7 +1041,8 @@ struct NewtonWork {
   double* x;      // nv planes: qj_rel while iterating, the final qj when done
   double* rt;     // nv planes: residual
   double* sf;     // 1 plane: 0.5*|residual|^2
-  uint8_t* status;  // 1 plane: 1 = the cell went through Newton
+  uint8_t* status;  // 1 plane: bit 0 the cell went through Newton, bit 1 its
+                    // residual must be evaluated again (see newton_iterk)
   uint32_t* list[3];  // cells (k*pitch + j) still iterating after pass 0, 1, 2
 };
 
@@ -1219,9 +1241,11 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
         rt[i] = W.rt[c + i * N];
       }
       scal_f = W.sf[c];
+      bool stale = (W.status[c] & 2) != 0;
       newton_scale<NS>(qj, qj_org);
       long long tr = 0;
-      bool done = newton_iterk<NS>(P, qj, q0, Rj, Bx[c], By[c], dt, qj_org, qj_rel, rt, scal_f, tr);
+      bool done = newton_iterk<NS>(P, qj, q0, Rj, Bx[c], By[c], dt, qj_org, qj_rel, rt, scal_f, tr,
+                                   stale);
       trials += (unsigned long long)tr;
       if (done || nl_iter >= NEWTON_MAX_IT) {
         fin = nl_iter;
@@ -1235,6 +1259,7 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
           W.rt[c + i * N] = rt[i];
         }
         W.sf[c] = scal_f;
+        W.status[c] = stale ? 3 : 1;
       }
     }
     newton_finish_stats(clk, fin, it_sum, maxit);
@@ -1272,12 +1297,14 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
         rt[i] = W.rt[c + i * N];
       }
       scal_f = W.sf[c];
+      bool stale = (W.status[c] & 2) != 0;
       newton_scale<NS>(qj, qj_org);
       const double bx = Bx[c], by = By[c];
       int it;
       for (it = 4; it <= NEWTON_MAX_IT; ++it) {
         long long tr = 0;
-        bool done = newton_iterk<NS>(P, qj, q0, Rj, bx, by, dt, qj_org, qj_rel, rt, scal_f, tr);
+        bool done = newton_iterk<NS>(P, qj, q0, Rj, bx, by, dt, qj_org, qj_rel, rt, scal_f, tr,
+                                     stale);
         trials += (unsigned long long)tr;
         if (done) break;
       }
@@ -1310,7 +1337,7 @@ __global__ void __launch_bounds__(STAGE2_THREADS)
     double qc[NV];
 #pragma unroll
     for (int i = 0; i < NV; ++i) qc[i] = W.x[c + i * N];
-    if (W.status[c]) {
+    if (W.status[c] & 1) {
       const double qs1 = W.qsi[c + N], qs2 = W.qsi[c + 2 * N];
       if (ny == 1) qc[2] = 0.0;
       if (nx == 1) qc[1] = 0.0;

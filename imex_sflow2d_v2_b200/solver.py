@@ -66,6 +66,16 @@ def load_library(path=LIB_PATH):
         "imex_gpu_kernel_times": ([vp, dp, i64p, C.c_int], C.c_int),
         "imex_gpu_measure_fp64_peak": ([C.c_int, dp], C.c_int),
         "imex_gpu_build_info": ([], C.c_char_p),
+        "imex_gpu_ensemble_create": ([C.c_int, C.POINTER(C.POINTER(ImexParams)),
+                                      C.POINTER(C.POINTER(ImexStatic)), C.c_int,
+                                      C.POINTER(vp)], C.c_int),
+        "imex_gpu_ensemble_destroy": ([vp], C.c_int),
+        "imex_gpu_ensemble_member": ([vp, C.c_int, C.POINTER(vp)], C.c_int),
+        "imex_gpu_ensemble_advance": ([vp, C.c_int, C.POINTER(C.c_int)], C.c_int),
+        "imex_gpu_ensemble_tuning": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                      C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int],
+                                     C.c_int),
+        "imex_gpu_ensemble_last_error": ([vp], C.c_char_p),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -92,11 +102,16 @@ def measure_fp64_peak(device=-1):
 class ImexSolver:
     """One device context holding the state of one run."""
 
-    def __init__(self, params, static_arrays, device=-1):
+    def __init__(self, params, static_arrays, device=-1, _handle=None):
         self.lib = load_library()
         self.params = params
         self.nx, self.ny, self.ns = params.nx, params.ny, params.n_solid
         self.nv = 4 + self.ns
+        self._owned = _handle is None
+        if _handle is not None:        # a member context owned by an ImexEnsemble
+            self._keep = []
+            self._h = _handle
+            return
         st, self._keep = make_static(static_arrays)
         h = C.c_void_p()
         rc = self.lib.imex_gpu_create(C.byref(params), C.byref(st), int(device), C.byref(h))
@@ -111,7 +126,8 @@ class ImexSolver:
 
     def close(self):
         if getattr(self, "_h", None):
-            self.lib.imex_gpu_destroy(self._h)
+            if getattr(self, "_owned", True):
+                self.lib.imex_gpu_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -239,3 +255,71 @@ class ImexSolver:
         self._check(self.lib.imex_gpu_device_state(self._h, C.byref(p), C.byref(pitch)),
                     "device_state")
         return C.cast(p, C.c_void_p).value, pitch.value
+
+
+class ImexEnsemble:
+    """Independent runs (members) advanced together on one GPU from one CUDA
+    graph per step (the reference runs one process per member,
+    EXAMPLES/EXAMPLE_ENSEMBLE_ETNA/launch_jobs.py).  `members` is a list of
+    (params, static_arrays); member m's context is ``self.member(m)`` (an
+    ImexSolver view for set_state, set_clock, get_state, stats ...)."""
+
+    def __init__(self, members, device=-1):
+        self.lib = load_library()
+        n = len(members)
+        self._keep = []
+        P = (C.POINTER(ImexParams) * n)()
+        S = (C.POINTER(ImexStatic) * n)()
+        for m, (params, static_arrays) in enumerate(members):
+            st, keep = make_static(static_arrays)
+            self._keep.append((params, st, keep))
+            P[m] = C.pointer(params)
+            S[m] = C.pointer(st)
+        h = C.c_void_p()
+        rc = self.lib.imex_gpu_ensemble_create(n, P, S, int(device), C.byref(h))
+        if rc != IMEX_OK:
+            raise ImexError(rc, "imex_gpu_ensemble_create")
+        self._h = h
+        self._views = []
+        for m, (params, _) in enumerate(members):
+            ch = C.c_void_p()
+            self.lib.imex_gpu_ensemble_member(self._h, m, C.byref(ch))
+            self._views.append(ImexSolver(params, None, _handle=ch))
+
+    def __len__(self):
+        return len(self._views)
+
+    def member(self, m):
+        return self._views[m]
+
+    def advance(self, n_steps):
+        """n_steps driver-loop passes of every member; returns (status, first
+        member with a non-zero status or -1)."""
+        bad = C.c_int(-1)
+        rc = self.lib.imex_gpu_ensemble_advance(self._h, int(n_steps), C.byref(bad))
+        if rc > 6:
+            raise ImexError(rc, "imex_gpu_ensemble_advance",
+                            self.lib.imex_gpu_ensemble_last_error(self._h).decode())
+        return rc, bad.value
+
+    def tuning(self):
+        """(chosen stream count, [(candidate, ms of its timed step), ...])."""
+        k = C.c_int(0)
+        n = C.c_int(0)
+        tk = (C.c_int * 16)()
+        tm = (C.c_float * 16)()
+        self.lib.imex_gpu_ensemble_tuning(self._h, C.byref(k), C.byref(n), tk, tm, 16)
+        return k.value, [(tk[i], tm[i]) for i in range(min(n.value, 16))]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            for v in self._views:
+                v._h = None
+            self.lib.imex_gpu_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

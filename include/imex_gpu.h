@@ -248,6 +248,36 @@ int imex_gpu_profile(ImexCtx* ctx, int enable);
 int imex_gpu_kernel_times(ImexCtx* ctx, double* total_ms, int64_t* launches, int n_kernels);
 int imex_gpu_measure_fp64_peak(int device, double* gflops);
 
+/*
+ * Ensembles: many independent runs (members), each with its own grid,
+ * parameters and static planes, advanced together on one GPU.  This replaces
+ * the reference's process-level ensemble (EXAMPLES/EXAMPLE_ENSEMBLE_ETNA:
+ * create_ensemble.py samples the inputs, launch_jobs.py:13-30 runs one
+ * single-threaded IMEX_SfloW2D process per member); the sampling of inputs
+ * stays with the caller.
+ *
+ * imex_gpu_ensemble_create makes one context per member (params[m],
+ * statics[m]).  imex_gpu_ensemble_member returns member m's context for the
+ * single-context calls (set_state, set_clock, get_state, get_exchange, stats,
+ * get_masks); do not call imex_gpu_advance or the per-routine calls on a
+ * member while the ensemble advances.  imex_gpu_ensemble_advance runs n_steps
+ * driver-loop passes (as imex_gpu_advance) of every member from one CUDA
+ * graph that forks the members over K streams; its first calls time one real
+ * step for K = 1, 2, 4, ... up to min(members, 32) and keep the fastest K
+ * (results do not depend on K).  It returns the first status code found
+ * (member order) and, in *first_bad_member, that member (-1: none).
+ * imex_gpu_ensemble_tuning reports the chosen K and the timed candidates.
+ */
+typedef struct ImexEnsemble ImexEnsemble;
+int imex_gpu_ensemble_create(int n_members, const ImexParams* const* params,
+                             const ImexStatic* const* statics, int device, ImexEnsemble** out);
+int imex_gpu_ensemble_destroy(ImexEnsemble* ens);
+int imex_gpu_ensemble_member(ImexEnsemble* ens, int m, ImexCtx** ctx);
+int imex_gpu_ensemble_advance(ImexEnsemble* ens, int n_steps, int* first_bad_member);
+int imex_gpu_ensemble_tuning(ImexEnsemble* ens, int* k_streams, int* n_tried, int* tried_k,
+                             float* tried_ms, int cap);
+const char* imex_gpu_ensemble_last_error(ImexEnsemble* ens);
+
 /* Build information: "sm_100a fmad=0 ..." */
 const char* imex_gpu_build_info(void);
 

@@ -129,3 +129,34 @@ def test_repeat_runs_are_bit_identical():
         g.advance(20, use_graph=True)
         out.append(g.get_state())
     np.testing.assert_array_equal(out[0], out[1])
+
+
+def test_ensemble_member_breakdown_bitexact():
+    """A member of the ensemble workload (341^2, 7.1e6 kg/s) whose current
+    reaches the west boundary: the reference's checks fire from step ~407
+    (T < 273 K, then solid sum, negative h), dt collapses and q turns NaN at
+    step ~466.  The CUDA path follows the oracle through all of it, step for
+    step (NaNs compared as equal, whatever their payload)."""
+    from imex_sflow2d_v2_b200 import configs
+    from imex_sflow2d_v2_b200.solver import ImexSolver
+    from oracle import Oracle
+    p, st, q, s = configs.ensemble_members(n_members=13)[12]
+    o = Oracle(p, st, threads=8)
+    g = ImexSolver(p, st)
+    for x in (o, g):
+        x.set_state(q, 0.0)
+        x.set_clock(0.0, 1e-2)
+    first_err = None
+    for step in range(1, 471):
+        eo, to = o.advance(1)
+        eg, tg = g.advance(1)
+        assert tg == to or (np.isnan(tg) and np.isnan(to)), step
+        so, sg = o.stats(), g.stats()
+        assert (so.error_mask, so.first_error_code, so.first_error_j, so.first_error_k) == \
+            (sg.error_mask, sg.first_error_code, sg.first_error_j, sg.first_error_k), step
+        if so.error_mask and first_err is None:
+            first_err = step
+        if step % 10 == 0 or step > 400:
+            assert np.array_equal(o.get_state(), g.get_state(), equal_nan=True), step
+    assert first_err is not None and first_err > 300
+    assert np.isnan(g.get_state()).any()
