@@ -137,3 +137,69 @@ def test2d():
           "erosion": np.zeros((nx, ny, 1))}
     st.update(configs.topography_geom(B, p.cell_size, p.cell_size))
     return p, st, np.asfortranarray(d["q"])
+
+
+def dambreak_ns(ns, nx=40, ny=40, dx=0.25, rheology=1):
+    """Dam break with `ns` solid classes (diameters 1e-5..1e-3 m)."""
+    p = configs.default_params(nx, ny, ns, dx)
+    for i in range(ns):
+        p.rho_s[i] = 2500.0 - 200.0 * i
+        p.diam_s[i] = 10.0 ** (-5 + 2.0 * i / max(ns - 1, 1))
+        p.sp_heat_s[i] = 1617.0
+    p.max_dt = 1.0e-2
+    configs.transmissive_bcs(p)
+    p.rheology_flag = 1
+    p.rheology_model = rheology
+    p.mu, p.xi = 0.1, 500.0
+    _, xc, _, _ = configs.grid(p)
+    h = np.where(np.repeat(xc[:, None], ny, axis=1) < 0.5 * nx * dx, 1.0, 0.1)
+    qp = np.zeros((4 + ns + 2, nx, ny))
+    qp[0] = h
+    qp[3] = 300.0
+    for i in range(ns):
+        qp[4 + i] = 0.01 / ns * h
+    zeros = np.zeros((nx, ny))
+    st = {"B_cent": zeros, "B_prime_x_geom": zeros, "B_prime_y_geom": zeros,
+          "solve_mask_time": zeros}
+    return p, st, configs.qp_to_qc_grid(p, qp)
+
+
+def edge_variants():
+    """Options and shapes beyond the workloads: the remaining limiters,
+    four solid classes, a rectangular grid with per-cell release times and a
+    Neumann slope on one side, no-data cells, an all-dry grid, the smallest
+    grid."""
+    out = {}
+    for lim in (0, 5, 6, 7):
+        p, st, q = dambreak(rheology=1)
+        for i in range(7):
+            p.limiter[i] = lim
+        out["limiter%d" % lim] = (p, st, q)
+    out["four_classes"] = dambreak_ns(4)
+    out["two_classes_quadratic"] = dambreak_ns(2, rheology=6)
+    # rectangular grid with ragged tiles; the dry strip east of x = 9.2 m is
+    # released at t = 0.05 s, as the front arrives; Neumann slope on h at E
+    p2, st2, q2 = configs.dambreak(nx=70, ny=33, dx=0.25, rheology=1, x_split=8.0)
+    _, xc, _, _ = configs.grid(p2)
+    X = np.repeat(xc[:, None], 33, axis=1)
+    st2 = dict(st2)
+    st2["solve_mask_time"] = np.asfortranarray(np.where(X > 9.2, 0.05, 0.0))
+    q2 = q2.copy()
+    q2[:, X > 9.2] = 0.0
+    configs.set_bc(p2, "E", 0, 1, 0.01)      # h: Neumann with a non-zero slope
+    out["rect_release_neumann"] = (p2, st2, q2)
+    # no-data patch inside the flow (the reference zeroes it after each step)
+    p, st, q = dambreak(rheology=1)
+    nd = np.zeros((p.nx, p.ny), np.int8)
+    nd[12:18, 20:30] = 1
+    st = dict(st)
+    st["B_nodata"] = nd
+    q = q.copy()
+    q[:, nd == 1] = 0.0
+    out["nodata_patch"] = (p, st, q)
+    # all dry: only the border rows are solved
+    p, st, q = dambreak(rheology=1)
+    out["all_dry"] = (p, st, np.zeros_like(q))
+    # smallest grid the path accepts
+    out["tiny_3x5"] = configs.dambreak(nx=3, ny=5, dx=0.25, rheology=1, x_split=0.4)
+    return out

@@ -160,3 +160,13 @@ def test_ensemble_member_breakdown_bitexact():
             assert np.array_equal(o.get_state(), g.get_state(), equal_nan=True), step
     assert first_err is not None and first_err > 300
     assert np.isnan(g.get_state()).any()
+
+
+EDGE = cases.edge_variants()
+
+
+@pytest.mark.parametrize("name", sorted(EDGE))
+def test_edge_variants_bitexact(name):
+    p, st, q = EDGE[name]
+    recs, o, g = lockstep(p, st, q, 20)
+    assert_bitexact(recs, allow_errors=True)
