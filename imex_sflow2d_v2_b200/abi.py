@@ -115,6 +115,23 @@ class ImexStats(C.Structure):
     ]
 
 
+class ImexPostDiag(C.Structure):
+    _fields_ = [("mass", C.c_double), ("volume", C.c_double), ("area", C.c_double),
+                ("solid_mass", C.c_double)]
+
+
+def vulnerability_levels(thickness_levels, dyn_pres_levels):
+    """read_param's rule for VULNERABILITY_TABLE_PARAMETERS
+    (src/inpout_2d.f90:3630-3682): one kind given alone makes the other a
+    single level 0."""
+    t, d = list(thickness_levels), list(dyn_pres_levels)
+    if t and not d:
+        d = [0.0]
+    if d and not t:
+        t = [0.0]
+    return t, d
+
+
 # static plane name -> (dtype, shape kind) ; shape kinds: "c" cell (nx,ny),
 # "sx" (nx+1,ny), "sy" (nx,ny+1), "e" (n_solid,nx,ny), "d" (nx,ny,n_solid)
 STATIC_FIELDS = {

@@ -277,7 +277,8 @@ IMEX_HD double sp_heat_c_of(const DevParams& P, const double* qpj, double rho_m)
 // ----------------------------------------------------------- qc_to_qp
 // r_phys_var + qc_to_qp; also returns red_grav through the out pointer.
 template <int NS>
-IMEX_NOINL void qc_to_qp(const DevParams& P, const double* qc, double* qp) {
+IMEX_NOINL void qc_to_qp(const DevParams& P, const double* qc, double* qp,
+                         double* p_dyn = nullptr) {
   constexpr int NV = 4 + NS;
   if (!(qc[0] > EPS)) {
     qp[0] = 0.0;
@@ -288,6 +289,7 @@ IMEX_NOINL void qc_to_qp(const DevParams& P, const double* qc, double* qp) {
     for (int i = 0; i < NS; ++i) qp[4 + i] = P.alpha_flag ? 0.0 : 0.0 * 0.0;
     qp[NV] = 0.0;
     qp[NV + 1] = 0.0;
+    if (p_dyn) *p_dyn = 0.0;
     return;
   }
   double inv_qj1 = 1.0 / qc[0];
@@ -353,6 +355,7 @@ IMEX_NOINL void qc_to_qp(const DevParams& P, const double* qc, double* qp) {
   }
   qp[NV] = u;
   qp[NV + 1] = v;
+  if (p_dyn) *p_dyn = 0.5 * rho_m * (u * u + v * v);  // r_phys_var's p_dyn
 }
 
 // The driver's convention for a cell's physical state: qc_to_qp when q1 > 0,

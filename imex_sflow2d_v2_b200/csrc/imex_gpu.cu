@@ -40,6 +40,13 @@ struct ImexCtx {
   DevClock* clk_host = nullptr;  // pinned mirror
   double* scratch = nullptr;     // AoS staging for transfers
   NewtonWork nw{};               // stage-2 Newton state between passes
+  // driver output sweep (imex_gpu_post_init): planes, levels, diag partials
+  bool post_on = false;
+  PostLevels post_levels{};
+  PostPlanes post{};
+  double* post_buf = nullptr;
+  uint32_t* post_vuln = nullptr;
+  double* post_diag = nullptr;
   double* nw_buf = nullptr;      // backing store of nw's FP64 planes
   uint32_t* nw_lists = nullptr;  // backing store of nw's three cell lists
   size_t scratch_bytes = 0;
@@ -224,6 +231,34 @@ cudaError_t launch_erosion(ImexCtx* ctx) {
   }
 }
 
+cudaError_t launch_post_sweep(ImexCtx* ctx, int init) {
+  const DevParams& P = ctx->P;
+  const int grid = grid_1d((long long)P.nx * P.ny, 128);
+  switch (ctx->ns) {
+    case 1: k_post_sweep<1><<<grid, 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->mask, ctx->post, ctx->post_levels, init); break;
+    case 2: k_post_sweep<2><<<grid, 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->mask, ctx->post, ctx->post_levels, init); break;
+    case 3: k_post_sweep<3><<<grid, 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->mask, ctx->post, ctx->post_levels, init); break;
+    default: k_post_sweep<4><<<grid, 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->mask, ctx->post, ctx->post_levels, init); break;
+  }
+  ctx->launches += 1;
+  return cudaGetLastError();
+}
+
+constexpr int DIAG_BLOCKS = 148 * 4;
+
+cudaError_t launch_post_diag(ImexCtx* ctx) {
+  double* part = ctx->post_diag + 4;
+  switch (ctx->ns) {
+    case 1: k_post_diag<1><<<DIAG_BLOCKS, DIAG_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->post.qp_h, part); break;
+    case 2: k_post_diag<2><<<DIAG_BLOCKS, DIAG_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->post.qp_h, part); break;
+    case 3: k_post_diag<3><<<DIAG_BLOCKS, DIAG_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->post.qp_h, part); break;
+    default: k_post_diag<4><<<DIAG_BLOCKS, DIAG_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->post.qp_h, part); break;
+  }
+  k_post_diag_fold<<<1, 32, 0, ctx->stream>>>(part, DIAG_BLOCKS, ctx->post_diag);
+  ctx->launches += 2;
+  return cudaGetLastError();
+}
+
 cudaError_t launch_mask(ImexCtx* ctx, int solve_all = 0) {
   const DevParams& P = ctx->P;
   k_mask<<<tile_grid(P), 256, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->release, ctx->cellinfo,
@@ -258,6 +293,7 @@ cudaError_t enqueue_step(ImexCtx* ctx) {
     ProfScope ps(ctx, KID_EROSION);
     if ((e = launch_erosion(ctx)) != cudaSuccess) return e;
   }
+  if (ctx->post_on && (e = launch_post_sweep(ctx, 0)) != cudaSuccess) return e;
   k_step_end<<<1, 1, 0, ctx->stream>>>(ctx->clk);
   ctx->launches += 1;
   return cudaGetLastError();
@@ -554,7 +590,8 @@ int imex_gpu_destroy(ImexCtx* ctx) {
   void* bufs[] = {ctx->q, ctx->X, ctx->mask, ctx->cellinfo, ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy,
                   ctx->Byy, ctx->gc, ctx->dgc, ctx->gcsx, ctx->gcsy, ctx->release, ctx->erodible,
                   ctx->deposit, ctx->erosion, ctx->Bcent, ctx->ring, ctx->clk, ctx->scratch, ctx->dP,
-                  ctx->nw_buf, ctx->nw.status, ctx->nw_lists};
+                  ctx->nw_buf, ctx->nw.status, ctx->nw_lists, ctx->post_buf, ctx->post_vuln,
+                  ctx->post_diag};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (ctx->clk_host) cudaFreeHost(ctx->clk_host);
@@ -912,6 +949,118 @@ int imex_gpu_device_state(ImexCtx* ctx, double** q_dev, int64_t* pitch) {
   if (!ctx) return IMEX_EINVAL;
   if (q_dev) *q_dev = ctx->q;
   if (pitch) *pitch = ctx->P.pitch;
+  return IMEX_OK;
+}
+
+}  // extern "C"
+
+// ============================================================ post step
+extern "C" {
+
+int imex_gpu_post_init(ImexCtx* ctx, int n_thickness_levels, const double* thickness_levels,
+                       int n_dyn_pres_levels, const double* dyn_pres_levels) {
+  if (!ctx) return IMEX_EINVAL;
+  int nt = std::max(n_thickness_levels, 0), np = std::max(n_dyn_pres_levels, 0);
+  if (nt > POST_MAX_LEVELS || np > POST_MAX_LEVELS || (nt && !thickness_levels) ||
+      (np && !dyn_pres_levels))
+    return fail(ctx, IMEX_EINVAL, "imex_gpu_post_init: at most 10 levels of each kind");
+  PostLevels L{};
+  for (int i = 0; i < nt; ++i) L.thk[i] = thickness_levels[i];
+  for (int i = 0; i < np; ++i) L.pdyn[i] = dyn_pres_levels[i];
+  for (int i = 0; i < nt; ++i)
+    if (!(L.thk[i] >= 0.0)) return fail(ctx, IMEX_EINVAL, "imex_gpu_post_init: negative thickness level");
+  for (int i = 0; i < np; ++i)
+    if (!(L.pdyn[i] >= 0.0)) return fail(ctx, IMEX_EINVAL, "imex_gpu_post_init: negative pressure level");
+  // one kind given alone: the other is a single level 0 (src/inpout_2d.f90:3630-3682)
+  if (nt > 0 && np == 0) { np = 1; L.pdyn[0] = 0.0; }
+  if (np > 0 && nt == 0) { nt = 1; L.thk[0] = 0.0; }
+  L.n_thk = nt;
+  L.n_pdyn = np;
+  L.n_words = (nt * np + 31) / 32;
+  CK(cudaSetDevice(ctx->device));
+  const size_t plane = (size_t)ctx->P.plane;
+  if (!ctx->post_buf) {
+    CK(dalloc(&ctx->post_buf, plane * 4));
+    CK(dalloc(&ctx->post_diag, 4 + 4 * (size_t)DIAG_BLOCKS));
+  }
+  if (ctx->post_vuln) {
+    cudaFree(ctx->post_vuln);
+    ctx->post_vuln = nullptr;
+  }
+  if (L.n_words) CK(dalloc(&ctx->post_vuln, plane * L.n_words));
+  ctx->post.qp_h = ctx->post_buf;
+  ctx->post.hmax = ctx->post_buf + plane;
+  ctx->post.pdynmax = ctx->post_buf + 2 * plane;
+  ctx->post.mvmax = ctx->post_buf + 3 * plane;
+  ctx->post.vuln = ctx->post_vuln;
+  ctx->post_levels = L;
+  CK(cudaMemsetAsync(ctx->post_buf, 0, plane * 4 * sizeof(double), ctx->stream));
+  if (ctx->post_vuln)
+    CK(cudaMemsetAsync(ctx->post_vuln, 0, plane * L.n_words * sizeof(uint32_t), ctx->stream));
+  CK(launch_post_sweep(ctx, 1));
+  // a captured step does not hold the sweep yet
+  if (ctx->graph_exec) { cudaGraphExecDestroy(ctx->graph_exec); ctx->graph_exec = nullptr; }
+  if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+  ctx->post_on = true;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return IMEX_OK;
+}
+
+int imex_gpu_post_diag(ImexCtx* ctx, ImexPostDiag* diag) {
+  if (!ctx || !diag) return IMEX_EINVAL;
+  if (!ctx->post_on) return fail(ctx, IMEX_EINVAL, "imex_gpu_post_diag: call imex_gpu_post_init first");
+  CK(cudaSetDevice(ctx->device));
+  CK(launch_post_diag(ctx));
+  double out[4];
+  CK(cudaMemcpyAsync(out, ctx->post_diag, sizeof(out), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  const double cell = ctx->P.dx * ctx->P.dy;
+  diag->mass = cell * out[0];
+  diag->volume = cell * out[1];
+  diag->area = cell * out[2];
+  diag->solid_mass = cell * out[3];
+  return IMEX_OK;
+}
+
+int imex_gpu_post_step(ImexCtx* ctx, ImexPostDiag* diag) {
+  if (!ctx) return IMEX_EINVAL;
+  if (!ctx->post_on) return fail(ctx, IMEX_EINVAL, "imex_gpu_post_step: call imex_gpu_post_init first");
+  CK(cudaSetDevice(ctx->device));
+  CK(launch_post_sweep(ctx, 0));
+  if (diag) return imex_gpu_post_diag(ctx, diag);
+  CK(cudaStreamSynchronize(ctx->stream));
+  return IMEX_OK;
+}
+
+int imex_gpu_get_post(ImexCtx* ctx, double* hmax, double* pdynmax, double* mod_vel_max,
+                      int8_t* vuln_table, int* n_table) {
+  if (!ctx) return IMEX_EINVAL;
+  if (!ctx->post_on) return fail(ctx, IMEX_EINVAL, "imex_gpu_get_post: call imex_gpu_post_init first");
+  CK(cudaSetDevice(ctx->device));
+  const DevParams& P = ctx->P;
+  const size_t nx = (size_t)P.nx, ny = (size_t)P.ny, pitch = (size_t)P.pitch;
+  double* planes[3] = {hmax, pdynmax, mod_vel_max};
+  const double* src[3] = {ctx->post.hmax, ctx->post.pdynmax, ctx->post.mvmax};
+  for (int i = 0; i < 3; ++i)
+    if (planes[i])
+      CK(cudaMemcpy2DAsync(planes[i], nx * sizeof(double), src[i], pitch * sizeof(double),
+                           nx * sizeof(double), ny, cudaMemcpyDeviceToHost, ctx->stream));
+  const int nt = ctx->post_levels.n_thk * ctx->post_levels.n_pdyn;
+  if (n_table) *n_table = nt;
+  if (vuln_table && nt) {
+    const int nw = ctx->post_levels.n_words;
+    std::vector<uint32_t> w(pitch * ny * nw);
+    CK(cudaMemcpyAsync(w.data(), ctx->post_vuln, w.size() * sizeof(uint32_t),
+                       cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (size_t k = 0; k < ny; ++k)
+      for (size_t j = 0; j < nx; ++j)
+        for (int i = 0; i < nt; ++i) {
+          uint32_t word = w[(size_t)(i >> 5) * pitch * ny + k * pitch + j];
+          vuln_table[(size_t)i + (size_t)nt * (j + nx * k)] = (int8_t)((word >> (i & 31)) & 1u);
+        }
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
   return IMEX_OK;
 }
 

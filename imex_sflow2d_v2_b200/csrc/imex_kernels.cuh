@@ -1543,6 +1543,128 @@ __global__ void k_qp_out(const DevParams* __restrict__ Pp, const double* __restr
   }
 }
 
+// ============================================================= post step
+// The driver's output sweep over the solve cells after each step
+// (src/IMEX_SfloW2D.f90:391-442) and its first form after the initial
+// check_solve (src/IMEX_SfloW2D.f90:253-309): qp(1) kept for the volume
+// print, the running maxima hmax / pdynmax / mod_vel_max, and the
+// vulnerability table vuln_table(i_table) = OR over steps of
+// (h >= thickness_levels(i_thk)) .AND. (p_dyn >= dyn_pres_levels(i_pdyn)),
+// i_table running over i_pdyn fastest.
+constexpr int POST_MAX_LEVELS = 10;
+constexpr int POST_MAX_WORDS = (POST_MAX_LEVELS * POST_MAX_LEVELS + 31) / 32;
+
+struct PostLevels {
+  int n_thk, n_pdyn, n_words, pad_;
+  double thk[POST_MAX_LEVELS], pdyn[POST_MAX_LEVELS];
+};
+
+struct PostPlanes {
+  double* qp_h;     // qp(1,:,:) as the sweep leaves it
+  double* hmax;
+  double* pdynmax;
+  double* mvmax;    // mod_vel_max
+  uint32_t* vuln;   // n_words planes; table entry i is bit i%32 of plane i/32
+};
+
+template <int NS>
+__global__ void __launch_bounds__(128)
+    k_post_sweep(const DevParams* __restrict__ Pp, const double* __restrict__ q,
+                 const uint8_t* __restrict__ mask, PostPlanes W, PostLevels L, int init) {
+  const DevParams& P = *Pp;
+  constexpr int NV = 4 + NS, NP = 6 + NS;
+  const long long ncell = (long long)P.nx * P.ny;
+  const size_t N = (size_t)P.plane;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < ncell;
+       g += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(g % P.nx), k = (int)(g / P.nx);
+    const size_t c = (size_t)k * P.pitch + j;
+    if (!mask[c]) continue;
+    double qc[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) qc[i] = q[c + i * N];
+    if (qc[0] > 0.0) {
+      double qpv[NP], pd;
+      qc_to_qp<NS>(P, qc, qpv, &pd);
+      const double h = qpv[0];
+      W.qp_h[c] = h;
+      W.hmax[c] = init ? h : fmax_f(W.hmax[c], h);
+      const double u = qpv[NV], v = qpv[NV + 1];
+      const double mv = sqrt(u * u + v * v);
+      if (h > 0.001) {
+        W.pdynmax[c] = init ? pd : fmax_f(W.pdynmax[c], pd);
+        W.mvmax[c] = init ? mv : fmax_f(W.mvmax[c], mv);
+      }
+      uint32_t bits[POST_MAX_WORDS] = {0, 0, 0, 0};
+      int it = 0;
+      for (int a = 0; a < L.n_thk; ++a) {
+        const bool thck = h >= L.thk[a];
+        for (int b = 0; b < L.n_pdyn; ++b, ++it)
+          if (thck && pd >= L.pdyn[b]) bits[it >> 5] |= 1u << (it & 31);
+      }
+      for (int w = 0; w < L.n_words; ++w) {
+        uint32_t* dst = W.vuln + (size_t)w * N + c;
+        *dst = init ? bits[w] : (*dst | bits[w]);
+      }
+    } else {
+      W.qp_h[c] = 0.0;
+      if (init) {
+        W.hmax[c] = 0.0;
+        W.pdynmax[c] = 0.0;
+      }
+    }
+  }
+}
+
+// The driver's per-step print (src/IMEX_SfloW2D.f90:476-484) before the
+// dx*dy factor: SUM(q(1,:,:)), SUM(qp(1,:,:)), COUNT(q(1,:,:) > 1e-7) and
+// SUM(q(5:4+n_solid,:,:)).  Per-block partial sums in a fixed order, then
+// one block folds them in block order, so the result does not vary from
+// run to run.
+constexpr int DIAG_THREADS = 256;
+template <int NS>
+__global__ void __launch_bounds__(DIAG_THREADS)
+    k_post_diag(const DevParams* __restrict__ Pp, const double* __restrict__ q,
+                const double* __restrict__ qp_h, double* __restrict__ part) {
+  const DevParams& P = *Pp;
+  const long long ncell = (long long)P.nx * P.ny;
+  const size_t N = (size_t)P.plane;
+  double a[4] = {0.0, 0.0, 0.0, 0.0};
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < ncell;
+       g += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(g % P.nx), k = (int)(g / P.nx);
+    const size_t c = (size_t)k * P.pitch + j;
+    const double h = q[c];
+    a[0] += h;
+    a[1] += qp_h[c];
+    a[2] += (h > 1.0e-7) ? 1.0 : 0.0;
+#pragma unroll
+    for (int i = 0; i < NS; ++i) a[3] += q[c + (size_t)(4 + i) * N];
+  }
+  __shared__ double red[4][DIAG_THREADS / 32];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    double x = a[r];
+    for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+    if ((threadIdx.x & 31) == 0) red[r][threadIdx.x >> 5] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double x = 0.0;
+    for (int w = 0; w < DIAG_THREADS / 32; ++w) x += red[threadIdx.x][w];
+    part[(size_t)blockIdx.x * 4 + threadIdx.x] = x;
+  }
+}
+
+__global__ void k_post_diag_fold(const double* __restrict__ part, int nblocks,
+                                 double* __restrict__ out) {
+  if (threadIdx.x < 4) {
+    double x = 0.0;
+    for (int b = 0; b < nblocks; ++b) x += part[(size_t)b * 4 + threadIdx.x];
+    out[threadIdx.x] = x;
+  }
+}
+
 // solve_mask_x / solve_mask_y from solve_mask (src/solver_2d.f90:779-808).
 __global__ void k_masks_xy(const DevParams* __restrict__ Pp, const uint8_t* __restrict__ mask, int8_t* mx,
                            int8_t* my) {

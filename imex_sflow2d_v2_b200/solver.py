@@ -14,8 +14,8 @@ import os
 
 import numpy as np
 
-from .abi import (IMEX_OK, STATUS_NAMES, ImexParams, ImexStatic, ImexStats,
-                  make_static)
+from .abi import (IMEX_OK, STATUS_NAMES, ImexParams, ImexPostDiag, ImexStatic,
+                  ImexStats, make_static)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libimexgpu.so")
@@ -66,6 +66,10 @@ def load_library(path=LIB_PATH):
         "imex_gpu_kernel_times": ([vp, dp, i64p, C.c_int], C.c_int),
         "imex_gpu_measure_fp64_peak": ([C.c_int, dp], C.c_int),
         "imex_gpu_build_info": ([], C.c_char_p),
+        "imex_gpu_post_init": ([vp, C.c_int, dp, C.c_int, dp], C.c_int),
+        "imex_gpu_post_step": ([vp, C.POINTER(ImexPostDiag)], C.c_int),
+        "imex_gpu_post_diag": ([vp, C.POINTER(ImexPostDiag)], C.c_int),
+        "imex_gpu_get_post": ([vp, dp, dp, dp, i8p, C.POINTER(C.c_int)], C.c_int),
         "imex_gpu_ensemble_create": ([C.c_int, C.POINTER(C.POINTER(ImexParams)),
                                       C.POINTER(C.POINTER(ImexStatic)), C.c_int,
                                       C.POINTER(vp)], C.c_int),
@@ -183,6 +187,43 @@ class ImexSolver:
         dt = C.c_double(0.0)
         self._check(self.lib.imex_gpu_timestep(self._h, C.byref(dt)), "timestep")
         return dt.value
+
+    # -- the driver's output sweep (src/IMEX_SfloW2D.f90:253-309, 391-485)
+    def post_init(self, thickness_levels=(), dyn_pres_levels=()):
+        """First output sweep with the VULNERABILITY_TABLE_PARAMETERS levels;
+        afterwards advance() sweeps after every step."""
+        tl = np.ascontiguousarray(thickness_levels, dtype=np.float64)
+        pl = np.ascontiguousarray(dyn_pres_levels, dtype=np.float64)
+        return self._check(self.lib.imex_gpu_post_init(self._h, len(tl), _p(tl), len(pl), _p(pl)),
+                           "post_init")
+
+    def post_step(self, diag=True):
+        """The sweep after one step taken with the per-routine calls; returns
+        the print values (mass, volume, area, solid_mass) when `diag`."""
+        d = ImexPostDiag()
+        self._check(self.lib.imex_gpu_post_step(self._h, C.byref(d) if diag else None),
+                    "post_step")
+        return (d.mass, d.volume, d.area, d.solid_mass) if diag else None
+
+    def post_diag(self):
+        d = ImexPostDiag()
+        self._check(self.lib.imex_gpu_post_diag(self._h, C.byref(d)), "post_diag")
+        return d.mass, d.volume, d.area, d.solid_mass
+
+    def get_post(self):
+        """(hmax, pdynmax, mod_vel_max) as (nx,ny) arrays and vuln_table as
+        (n_table,nx,ny) 0/1 bytes."""
+        n = self.nx * self.ny
+        a = [np.zeros(n) for _ in range(3)]
+        nt = C.c_int(0)
+        self._check(self.lib.imex_gpu_get_post(self._h, None, None, None, None, C.byref(nt)),
+                    "get_post")
+        v = np.zeros(max(nt.value, 1) * n, np.int8)
+        self._check(self.lib.imex_gpu_get_post(self._h, _p(a[0]), _p(a[1]), _p(a[2]),
+                                               v.ctypes.data_as(C.POINTER(C.c_int8)),
+                                               C.byref(nt)), "get_post")
+        f = [x.reshape((self.nx, self.ny), order="F") for x in a]
+        return f[0], f[1], f[2], v[:nt.value * n].reshape((nt.value, self.nx, self.ny), order="F")
 
     def timestep_noalloc(self):
         """CFL dt like timestep(), through the entry point that allocates

@@ -249,6 +249,35 @@ int imex_gpu_kernel_times(ImexCtx* ctx, double* total_ms, int64_t* launches, int
 int imex_gpu_measure_fp64_peak(int device, double* gflops);
 
 /*
+ * The driver's output sweep after each step on the device
+ * (src/IMEX_SfloW2D.f90:391-485, first form :253-309): qp(1) for the
+ * volume print, the running maxima hmax, pdynmax and mod_vel_max, the
+ * vulnerability table, and the per-step mass / volume / area / solid-mass
+ * print.  imex_gpu_post_init takes the VULNERABILITY_TABLE_PARAMETERS levels
+ * (at most 10 of each kind, none negative; one kind given alone makes the
+ * other a single level 0, as read_param does), zeroes the fields and runs the
+ * first sweep over the current solve cells; call it right after
+ * imex_gpu_set_state, as the driver runs its sweep right after the first
+ * check_solve.  From then on imex_gpu_advance runs the sweep after every
+ * step (also inside its CUDA graph); callers of the per-routine entry points
+ * call imex_gpu_post_step after the step.  imex_gpu_post_diag returns the
+ * driver's print values (dx*dy times the sums; area counts q(1) > 1e-7);
+ * its sums are taken in a fixed order on the device, so they equal the
+ * reference's sequential SUM to rounding, not bit for bit.
+ * imex_gpu_get_post writes hmax, pdynmax, mod_vel_max (nx,ny) and
+ * vuln_table (n_table,nx,ny) as 0/1 bytes; any pointer may be NULL.
+ */
+typedef struct ImexPostDiag {
+  double mass, volume, area, solid_mass;
+} ImexPostDiag;
+int imex_gpu_post_init(ImexCtx* ctx, int n_thickness_levels, const double* thickness_levels,
+                       int n_dyn_pres_levels, const double* dyn_pres_levels);
+int imex_gpu_post_step(ImexCtx* ctx, ImexPostDiag* diag /* NULL: no print values */);
+int imex_gpu_post_diag(ImexCtx* ctx, ImexPostDiag* diag);
+int imex_gpu_get_post(ImexCtx* ctx, double* hmax, double* pdynmax, double* mod_vel_max,
+                      int8_t* vuln_table, int* n_table);
+
+/*
  * Ensembles: many independent runs (members), each with its own grid,
  * parameters and static planes, advanced together on one GPU.  This replaces
  * the reference's process-level ensemble (EXAMPLES/EXAMPLE_ENSEMBLE_ETNA:

@@ -324,6 +324,13 @@ struct OracleCtx {
   uint32_t update_erosion_deposition_cell(double dtl);
   void post_step_sweep();
   void initial_sweep();
+  // driver output sweep (src/IMEX_SfloW2D.f90:253-309, 391-442)
+  bool post_on = false;
+  int n_thk = 0, n_pdyn = 0;
+  double thk_lev[10], pdyn_lev[10];
+  std::vector<double> hmax, pdynmax, mvmax;
+  std::vector<uint8_t> vuln;  // (n_thk*n_pdyn, cell)
+  void post_cell(int j, int k, bool init);
 };
 
 // ------------------------------------------------------------------ mixt_var
@@ -2028,6 +2035,10 @@ uint32_t OracleCtx::update_erosion_deposition_cell(double dtl) {
 
 // src/IMEX_SfloW2D.f90:391-447 (qp part; max tables are outside the step)
 void OracleCtx::post_step_sweep() {
+  if (post_on) {
+    for (int64_t l = 0; l < solve_cells; ++l) post_cell(j_cent[l], k_cent[l], false);
+    return;
+  }
   for (int64_t l = 0; l < solve_cells; ++l) {
     int j = j_cent[l], k = k_cent[l];
     double pd;
@@ -2037,6 +2048,42 @@ void OracleCtx::post_step_sweep() {
       double* o = QP(qp, j, k);
       for (int i = 0; i < np; ++i) o[i] = 0.0;
       o[3] = p.T_ambient;
+    }
+  }
+}
+
+// One cell of the driver's output sweep: qp, running maxima and the
+// vulnerability table (src/IMEX_SfloW2D.f90:398-440; init: :261-307).
+void OracleCtx::post_cell(int j, int k, bool init) {
+  const size_t c = c2(j, k);
+  if (Q(q, j, k)[0] > 0.0) {
+    double pd;
+    double* o = QP(qp, j, k);
+    qc_to_qp(Q(q, j, k), o, pd);
+    hmax[c] = init ? o[0] : fmax_f(hmax[c], o[0]);
+    double r_u = o[idx_u], r_v = o[idx_v];
+    double mod_vel = std::sqrt(r_u * r_u + r_v * r_v);
+    if (o[0] > 0.001) {
+      pdynmax[c] = init ? pd : fmax_f(pdynmax[c], pd);
+      mvmax[c] = init ? mod_vel : fmax_f(mvmax[c], mod_vel);
+    }
+    int it = 0, nt = n_thk * n_pdyn;
+    for (int a = 0; a < n_thk; ++a) {
+      bool thck = o[0] >= thk_lev[a];
+      for (int b = 0; b < n_pdyn; ++b, ++it) {
+        bool pdyn = pd >= pdyn_lev[b];
+        uint8_t& v = vuln[(size_t)it + (size_t)nt * c];
+        v = init ? (uint8_t)(thck && pdyn) : (uint8_t)(v || (thck && pdyn));
+      }
+    }
+  } else {
+    double* o = QP(qp, j, k);
+    // the first sweep clears qp(1:n_vars), the per-step one qp(1:n_vars+2)
+    for (int i = 0; i < (init ? nv : np); ++i) o[i] = 0.0;
+    o[3] = p.T_ambient;
+    if (init) {
+      hmax[c] = 0.0;
+      pdynmax[c] = 0.0;
     }
   }
 }
@@ -2396,3 +2443,49 @@ double oracle_limit(double v1, double v2, double v3, double z1, double z2, doubl
 }
 
 }  // extern "C"
+
+// Driver output sweep and print values (test infrastructure for the GPU's
+// imex_gpu_post_*): levels already normalised by the caller.
+extern "C" void oracle_post_init(OracleCtx* o, int n_thk, const double* thk, int n_pdyn,
+                                 const double* pdyn) {
+  o->n_thk = n_thk;
+  o->n_pdyn = n_pdyn;
+  for (int i = 0; i < n_thk; ++i) o->thk_lev[i] = thk[i];
+  for (int i = 0; i < n_pdyn; ++i) o->pdyn_lev[i] = pdyn[i];
+  const size_t N = (size_t)o->nx * o->ny;
+  o->hmax.assign(N, 0.0);
+  o->pdynmax.assign(N, 0.0);
+  o->mvmax.assign(N, 0.0);
+  o->vuln.assign(N * (size_t)(n_thk * n_pdyn), 0);
+  for (int64_t l = 0; l < o->solve_cells; ++l) o->post_cell(o->j_cent[l], o->k_cent[l], true);
+  o->post_on = true;
+}
+
+// SUM(q(1,:,:)), SUM(qp(1,:,:)), COUNT(q(1,:,:) > 1e-7), SUM(q(5:4+n_solid,:,:))
+// in array element order, times dx*dy (src/IMEX_SfloW2D.f90:476-484).
+extern "C" void oracle_post_diag(OracleCtx* o, double* out) {
+  const size_t N = (size_t)o->nx * o->ny;
+  double m = 0.0, v = 0.0, a = 0.0, sm = 0.0;
+  for (size_t c = 0; c < N; ++c) m += o->q[c * o->nv];
+  for (size_t c = 0; c < N; ++c) v += o->qp[c * o->np];
+  for (size_t c = 0; c < N; ++c) a += (o->q[c * o->nv] > 1.0e-7) ? 1.0 : 0.0;
+  for (size_t c = 0; c < N; ++c)
+    for (int i = 4; i < o->nv; ++i) sm += o->q[c * o->nv + i];
+  const double cell = o->dx * o->dy;
+  out[0] = cell * m;
+  out[1] = cell * v;
+  out[2] = cell * a;
+  out[3] = cell * sm;
+}
+
+extern "C" void oracle_get_post(OracleCtx* o, double* hmax, double* pdynmax, double* mvmax,
+                                int8_t* vuln) {
+  const size_t N = (size_t)o->nx * o->ny;
+  for (size_t c = 0; c < N; ++c) {
+    if (hmax) hmax[c] = o->hmax[c];
+    if (pdynmax) pdynmax[c] = o->pdynmax[c];
+    if (mvmax) mvmax[c] = o->mvmax[c];
+  }
+  if (vuln)
+    for (size_t i = 0; i < o->vuln.size(); ++i) vuln[i] = (int8_t)o->vuln[i];
+}

@@ -65,6 +65,9 @@ def lib():
                                            C.c_double, C.c_double]
         L.oracle_ipow.restype = C.c_double
         L.oracle_ipow.argtypes = [C.c_double, C.c_double]
+        L.oracle_post_init.argtypes = [vp, C.c_int, dp, C.c_int, dp]
+        L.oracle_post_diag.argtypes = [vp, dp]
+        L.oracle_get_post.argtypes = [vp, dp, dp, dp, C.POINTER(C.c_int8)]
         L.oracle_limit.restype = C.c_double
         L.oracle_limit.argtypes = [C.c_double] * 6 + [C.c_int, C.c_double]
         _LIB = L
@@ -160,6 +163,29 @@ class Oracle:
 
     def stale_wet_reads(self):
         return lib().oracle_stale_wet_reads(self._h)
+
+    # the driver's output sweep
+    def post_init(self, thickness_levels=(), dyn_pres_levels=()):
+        from imex_sflow2d_v2_b200.abi import vulnerability_levels
+        t, d = vulnerability_levels(thickness_levels, dyn_pres_levels)
+        self._nt = len(t) * len(d)
+        t = np.ascontiguousarray(t, dtype=np.float64)
+        d = np.ascontiguousarray(d, dtype=np.float64)
+        lib().oracle_post_init(self._h, len(t), _p(t), len(d), _p(d))
+
+    def post_diag(self):
+        out = np.zeros(4)
+        lib().oracle_post_diag(self._h, _p(out))
+        return tuple(out)
+
+    def get_post(self):
+        n = self.nx * self.ny
+        a = [np.zeros(n) for _ in range(3)]
+        v = np.zeros(max(self._nt, 1) * n, np.int8)
+        lib().oracle_get_post(self._h, _p(a[0]), _p(a[1]), _p(a[2]),
+                              v.ctypes.data_as(C.POINTER(C.c_int8)))
+        f = [x.reshape((self.nx, self.ny), order="F") for x in a]
+        return f[0], f[1], f[2], v[:self._nt * n].reshape((self._nt, self.nx, self.ny), order="F")
 
     # point functions
     def qc_to_qp(self, qc):

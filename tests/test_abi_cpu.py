@@ -46,8 +46,9 @@ def _c_layout():
 #include "imex_gpu.h"
 #define OFF(T, f) printf(#T "." #f " %zu\n", offsetof(T, f))
 int main(void) {
-  printf("ImexParams %zu\nImexStatic %zu\nImexStats %zu\nImexBC %zu\n", sizeof(ImexParams),
-         sizeof(ImexStatic), sizeof(ImexStats), sizeof(ImexBC));
+  printf("ImexParams %zu\nImexStatic %zu\nImexStats %zu\nImexBC %zu\nImexPostDiag %zu\n",
+         sizeof(ImexParams), sizeof(ImexStatic), sizeof(ImexStats), sizeof(ImexBC),
+         sizeof(ImexPostDiag));
   OFF(ImexParams, limiter); OFF(ImexParams, cfl); OFF(ImexParams, bcW); OFF(ImexParams, bcN);
   OFF(ImexParams, grav); OFF(ImexParams, rho_s); OFF(ImexParams, time_param);
   OFF(ImexParams, erodible_fract); OFF(ImexParams, coeff_porosity);
@@ -74,6 +75,7 @@ def test_ctypes_mirror_matches_c_layout():
     assert c["ImexStatic"] == C.sizeof(abi.ImexStatic)
     assert c["ImexStats"] == C.sizeof(abi.ImexStats)
     assert c["ImexBC"] == C.sizeof(abi.ImexBC)
+    assert c["ImexPostDiag"] == C.sizeof(abi.ImexPostDiag)
     for key, v in c.items():
         if "." in key:
             t, f = key.split(".")
