@@ -9,7 +9,7 @@ LIB = os.path.join(_HERE, "libimexgpu.so")
 
 
 def sources():
-    return [os.path.join(CSRC, f) for f in ("imex_gpu.cu", "imex_kernels.cuh",
+    return [os.path.join(CSRC, f) for f in ("imex_gpu.cu", "imex_kernels.cuh", "imex_mlp.cuh",
                                              "imex_device.cuh")] + [
         os.path.join(_HERE, "..", "include", "imex_gpu.h")]
 

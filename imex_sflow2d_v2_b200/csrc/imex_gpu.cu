@@ -15,6 +15,7 @@
 
 #include "../../include/imex_gpu.h"
 #include "imex_kernels.cuh"
+#include "imex_mlp.cuh"
 
 using namespace imex;
 
@@ -1063,6 +1064,238 @@ int imex_gpu_get_post(ImexCtx* ctx, double* hmax, double* pdynmax, double* mod_v
   CK(cudaStreamSynchronize(ctx->stream));
   return IMEX_OK;
 }
+
+}  // extern "C"
+
+// =================================================================== MLP
+struct ImexMLP {
+  int device = 0;
+  float* prm = nullptr;        // FP32 master parameters
+  float* grad = nullptr;
+  float* m1 = nullptr;
+  float* m2 = nullptr;
+  float* loss = nullptr;       // summed squared error of the last pass
+  __nv_bfloat16* bw = nullptr; // BF16 weights
+  int64_t adam_t = 0;
+  float norm[2 * mlp::IN + 2 * mlp::OUT] = {};  // x mean, x std, y mean, y std
+  std::string last_error;
+};
+
+namespace {
+
+int mlp_fail(ImexMLP* m, int code, const std::string& msg) {
+  if (m) m->last_error = msg;
+  return code;
+}
+#define CKM(call)                                                             \
+  do {                                                                        \
+    cudaError_t e_ = (call);                                                  \
+    if (e_ != cudaSuccess) return mlp_fail(mlp, IMEX_ECUDA, cudaGetErrorString(e_)); \
+  } while (0)
+
+uint64_t splitmix64(uint64_t& s) {
+  uint64_t z = (s += 0x9E3779B97F4A7C15ULL);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+double uniform01(uint64_t& s) { return (double)(splitmix64(s) >> 11) * (1.0 / 9007199254740992.0); }
+
+int mlp_refresh_bf16(ImexMLP* mlp) {
+  mlp::k_mlp_to_bf16<<<(mlp::NBW + 255) / 256, 256>>>(mlp->prm, mlp->bw);
+  CKM(cudaGetLastError());
+  return IMEX_OK;
+}
+
+int mlp_grad_pass(ImexMLP* mlp, const float* x, const float* y, long long n) {
+  static bool attr = false;
+  if (!attr) {
+    CKM(cudaFuncSetAttribute(mlp::k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)mlp::SMEM_GRAD));
+    attr = true;
+  }
+  const long long tiles = (n + mlp::SAMPLES - 1) / mlp::SAMPLES;
+  const int grid = (int)std::max<long long>(1, std::min<long long>(tiles, 148));
+  CKM(cudaMemset(mlp->loss, 0, sizeof(float)));
+  mlp::k_mlp_grad<<<grid, 32 * mlp::WARPS, mlp::SMEM_GRAD>>>(
+      mlp->bw, mlp->prm, x, y, n, 1.0f / (float)(n * mlp::OUT), mlp->grad, mlp->loss);
+  CKM(cudaGetLastError());
+  return IMEX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int imex_mlp_create(int device, uint64_t seed, ImexMLP** out) {
+  if (!out) return IMEX_EINVAL;
+  *out = nullptr;
+  ImexMLP* mlp = new ImexMLP();
+  if (device >= 0) CKM(cudaSetDevice(device));
+  CKM(cudaGetDevice(&mlp->device));
+  // He-uniform weights on the real rows/columns, zero padding and biases
+  std::vector<float> p(mlp::NPARAM, 0.0f);
+  uint64_t st = seed;
+  auto fill = [&](int off, int rows, int cols, int real_rows, int real_cols) {
+    const double a = std::sqrt(6.0 / real_rows);
+    for (int r = 0; r < real_rows; ++r)
+      for (int c = 0; c < real_cols; ++c) p[off + r * cols + c] = (float)((2.0 * uniform01(st) - 1.0) * a);
+    (void)rows;
+  };
+  fill(mlp::OFF_W0, mlp::IN_P, mlp::HID, mlp::IN, mlp::HID);
+  fill(mlp::OFF_W1, mlp::HID, mlp::HID, mlp::HID, mlp::HID);
+  fill(mlp::OFF_W2, mlp::HID, mlp::HID, mlp::HID, mlp::HID);
+  fill(mlp::OFF_W3, mlp::HID, mlp::OUT_P, mlp::HID, mlp::OUT);
+  CKM(cudaMalloc((void**)&mlp->prm, mlp::NPARAM * sizeof(float)));
+  CKM(cudaMalloc((void**)&mlp->grad, mlp::NPARAM * sizeof(float)));
+  CKM(cudaMalloc((void**)&mlp->m1, mlp::NPARAM * sizeof(float)));
+  CKM(cudaMalloc((void**)&mlp->m2, mlp::NPARAM * sizeof(float)));
+  CKM(cudaMalloc((void**)&mlp->loss, sizeof(float)));
+  CKM(cudaMalloc((void**)&mlp->bw, mlp::NBW * sizeof(__nv_bfloat16)));
+  CKM(cudaMemcpy(mlp->prm, p.data(), p.size() * sizeof(float), cudaMemcpyHostToDevice));
+  CKM(cudaMemset(mlp->grad, 0, mlp::NPARAM * sizeof(float)));
+  CKM(cudaMemset(mlp->m1, 0, mlp::NPARAM * sizeof(float)));
+  CKM(cudaMemset(mlp->m2, 0, mlp::NPARAM * sizeof(float)));
+  for (int i = 0; i < mlp::IN; ++i) mlp->norm[mlp::IN + i] = 1.0f;
+  for (int i = 0; i < mlp::OUT; ++i) mlp->norm[2 * mlp::IN + mlp::OUT + i] = 1.0f;
+  int r = mlp_refresh_bf16(mlp);
+  if (r) return r;
+  CKM(cudaDeviceSynchronize());
+  *out = mlp;
+  return IMEX_OK;
+}
+
+int imex_mlp_destroy(ImexMLP* mlp) {
+  if (!mlp) return IMEX_EINVAL;
+  cudaSetDevice(mlp->device);
+  void* b[] = {mlp->prm, mlp->grad, mlp->m1, mlp->m2, mlp->loss, mlp->bw};
+  for (void* x : b)
+    if (x) cudaFree(x);
+  delete mlp;
+  return IMEX_OK;
+}
+
+int imex_mlp_get_params(ImexMLP* mlp, float* params) {
+  if (!mlp || !params) return IMEX_EINVAL;
+  CKM(cudaSetDevice(mlp->device));
+  CKM(cudaMemcpy(params, mlp->prm, mlp::NPARAM * sizeof(float), cudaMemcpyDeviceToHost));
+  return IMEX_OK;
+}
+
+int imex_mlp_set_params(ImexMLP* mlp, const float* params) {
+  if (!mlp || !params) return IMEX_EINVAL;
+  CKM(cudaSetDevice(mlp->device));
+  CKM(cudaMemcpy(mlp->prm, params, mlp::NPARAM * sizeof(float), cudaMemcpyHostToDevice));
+  int r = mlp_refresh_bf16(mlp);
+  if (r) return r;
+  CKM(cudaDeviceSynchronize());
+  return IMEX_OK;
+}
+
+int imex_mlp_set_norm(ImexMLP* mlp, const float* norm) {
+  if (!mlp || !norm) return IMEX_EINVAL;
+  for (int i = 0; i < 2 * mlp::IN + 2 * mlp::OUT; ++i) mlp->norm[i] = norm[i];
+  return IMEX_OK;
+}
+
+int imex_mlp_get_norm(ImexMLP* mlp, float* norm) {
+  if (!mlp || !norm) return IMEX_EINVAL;
+  for (int i = 0; i < 2 * mlp::IN + 2 * mlp::OUT; ++i) norm[i] = mlp->norm[i];
+  return IMEX_OK;
+}
+
+int imex_mlp_predict(ImexMLP* mlp, const float* x, int64_t n, float* y) {
+  if (!mlp || !x || !y || n < 0) return IMEX_EINVAL;
+  if (n == 0) return IMEX_OK;
+  CKM(cudaSetDevice(mlp->device));
+  float *dx = nullptr, *dy = nullptr;
+  CKM(cudaMalloc((void**)&dx, n * mlp::IN * sizeof(float)));
+  CKM(cudaMalloc((void**)&dy, n * mlp::OUT * sizeof(float)));
+  CKM(cudaMemcpy(dx, x, n * mlp::IN * sizeof(float), cudaMemcpyHostToDevice));
+  CKM(cudaFuncSetAttribute(mlp::k_mlp_predict, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)mlp::SMEM_NET));
+  const long long tiles = (n + mlp::SAMPLES - 1) / mlp::SAMPLES;
+  mlp::k_mlp_predict<<<(int)std::min<long long>(tiles, 148 * 4), 32 * mlp::WARPS, mlp::SMEM_NET>>>(
+      mlp->bw, mlp->prm, dx, dy, n);
+  CKM(cudaGetLastError());
+  CKM(cudaMemcpy(y, dy, n * mlp::OUT * sizeof(float), cudaMemcpyDeviceToHost));
+  cudaFree(dx);
+  cudaFree(dy);
+  return IMEX_OK;
+}
+
+int imex_mlp_loss_grad(ImexMLP* mlp, const float* x, const float* y, int64_t n, float* loss,
+                       float* grad) {
+  if (!mlp || !x || !y || n <= 0) return IMEX_EINVAL;
+  CKM(cudaSetDevice(mlp->device));
+  float *dx = nullptr, *dy = nullptr;
+  CKM(cudaMalloc((void**)&dx, n * mlp::IN * sizeof(float)));
+  CKM(cudaMalloc((void**)&dy, n * mlp::OUT * sizeof(float)));
+  CKM(cudaMemcpy(dx, x, n * mlp::IN * sizeof(float), cudaMemcpyHostToDevice));
+  CKM(cudaMemcpy(dy, y, n * mlp::OUT * sizeof(float), cudaMemcpyHostToDevice));
+  CKM(cudaMemset(mlp->grad, 0, mlp::NPARAM * sizeof(float)));
+  int r = mlp_grad_pass(mlp, dx, dy, n);
+  if (r) return r;
+  float ls = 0.0f;
+  CKM(cudaMemcpy(&ls, mlp->loss, sizeof(float), cudaMemcpyDeviceToHost));
+  if (loss) *loss = ls / (float)(n * mlp::OUT);
+  if (grad) CKM(cudaMemcpy(grad, mlp->grad, mlp::NPARAM * sizeof(float), cudaMemcpyDeviceToHost));
+  CKM(cudaMemset(mlp->grad, 0, mlp::NPARAM * sizeof(float)));
+  cudaFree(dx);
+  cudaFree(dy);
+  return IMEX_OK;
+}
+
+// Adam on mini-batches of a device-resident training set (normalised x, y),
+// shuffled once with `seed`; loss_out[e] = mean squared error of epoch e.
+int imex_mlp_train(ImexMLP* mlp, const float* x_dev, const float* y_dev, int64_t n, int epochs,
+                   int batch, float lr, uint64_t seed, float* loss_out) {
+  if (!mlp || !x_dev || !y_dev || n <= 0 || epochs < 0 || batch <= 0) return IMEX_EINVAL;
+  CKM(cudaSetDevice(mlp->device));
+  std::vector<long long> perm(n);
+  for (long long i = 0; i < n; ++i) perm[i] = i;
+  uint64_t st = seed;
+  for (long long i = n - 1; i > 0; --i) {
+    long long j = (long long)(splitmix64(st) % (uint64_t)(i + 1));
+    std::swap(perm[i], perm[j]);
+  }
+  long long* dperm = nullptr;
+  float *xs = nullptr, *ys = nullptr;
+  CKM(cudaMalloc((void**)&dperm, n * sizeof(long long)));
+  CKM(cudaMalloc((void**)&xs, n * mlp::IN * sizeof(float)));
+  CKM(cudaMalloc((void**)&ys, n * mlp::OUT * sizeof(float)));
+  CKM(cudaMemcpy(dperm, perm.data(), n * sizeof(long long), cudaMemcpyHostToDevice));
+  mlp::k_gather_rows<<<148 * 8, 256>>>(x_dev, dperm, xs, n, mlp::IN);
+  mlp::k_gather_rows<<<148 * 8, 256>>>(y_dev, dperm, ys, n, mlp::OUT);
+  CKM(cudaGetLastError());
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  for (int e = 0; e < epochs; ++e) {
+    double esum = 0.0;
+    for (long long b0 = 0; b0 < n; b0 += batch) {
+      const long long nb = std::min<long long>(batch, n - b0);
+      int r = mlp_grad_pass(mlp, xs + b0 * mlp::IN, ys + b0 * mlp::OUT, nb);
+      if (r) return r;
+      ++mlp->adam_t;
+      const float c1 = 1.0f - std::pow(b1, (float)mlp->adam_t);
+      const float c2 = 1.0f - std::pow(b2, (float)mlp->adam_t);
+      mlp::k_mlp_adam<<<(mlp::NPARAM + 255) / 256, 256>>>(mlp->prm, mlp->grad, mlp->m1, mlp->m2,
+                                                           lr, b1, b2, eps, c1, c2);
+      r = mlp_refresh_bf16(mlp);
+      if (r) return r;
+      float ls = 0.0f;
+      CKM(cudaMemcpy(&ls, mlp->loss, sizeof(float), cudaMemcpyDeviceToHost));
+      esum += ls;
+    }
+    if (loss_out) loss_out[e] = (float)(esum / (double)(n * mlp::OUT));
+  }
+  CKM(cudaDeviceSynchronize());
+  cudaFree(dperm);
+  cudaFree(xs);
+  cudaFree(ys);
+  return IMEX_OK;
+}
+
+const char* imex_mlp_last_error(ImexMLP* mlp) { return mlp ? mlp->last_error.c_str() : "null"; }
 
 }  // extern "C"
 

@@ -70,6 +70,18 @@ def load_library(path=LIB_PATH):
         "imex_gpu_post_step": ([vp, C.POINTER(ImexPostDiag)], C.c_int),
         "imex_gpu_post_diag": ([vp, C.POINTER(ImexPostDiag)], C.c_int),
         "imex_gpu_get_post": ([vp, dp, dp, dp, i8p, C.POINTER(C.c_int)], C.c_int),
+        "imex_mlp_create": ([C.c_int, C.c_uint64, C.POINTER(vp)], C.c_int),
+        "imex_mlp_destroy": ([vp], C.c_int),
+        "imex_mlp_get_params": ([vp, C.POINTER(C.c_float)], C.c_int),
+        "imex_mlp_set_params": ([vp, C.POINTER(C.c_float)], C.c_int),
+        "imex_mlp_set_norm": ([vp, C.POINTER(C.c_float)], C.c_int),
+        "imex_mlp_get_norm": ([vp, C.POINTER(C.c_float)], C.c_int),
+        "imex_mlp_predict": ([vp, C.POINTER(C.c_float), C.c_int64, C.POINTER(C.c_float)], C.c_int),
+        "imex_mlp_loss_grad": ([vp, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int64,
+                                C.POINTER(C.c_float), C.POINTER(C.c_float)], C.c_int),
+        "imex_mlp_train": ([vp, vp, vp, C.c_int64, C.c_int, C.c_int, C.c_float, C.c_uint64,
+                            C.POINTER(C.c_float)], C.c_int),
+        "imex_mlp_last_error": ([vp], C.c_char_p),
         "imex_gpu_ensemble_create": ([C.c_int, C.POINTER(C.POINTER(ImexParams)),
                                       C.POINTER(C.POINTER(ImexStatic)), C.c_int,
                                       C.POINTER(vp)], C.c_int),
@@ -357,6 +369,84 @@ class ImexEnsemble:
             for v in self._views:
                 v._h = None
             self.lib.imex_gpu_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class ImexMLP:
+    """The warm-start network (12 -> 64 -> 64 -> 64 -> 2, SiLU; BF16 weights on
+    tensor cores, FP32 accumulate) with its training kernels."""
+
+    N_IN, N_OUT = 12, 2
+    NPARAM = 16 * 64 + 64 + 2 * (64 * 64 + 64) + 64 * 8 + 8
+
+    def __init__(self, seed=1, device=-1):
+        self.lib = load_library()
+        h = C.c_void_p()
+        rc = self.lib.imex_mlp_create(int(device), int(seed), C.byref(h))
+        if rc != IMEX_OK:
+            raise ImexError(rc, "imex_mlp_create")
+        self._h = h
+
+    def _check(self, rc, where):
+        if rc != IMEX_OK:
+            raise ImexError(rc, where, self.lib.imex_mlp_last_error(self._h).decode())
+
+    def params(self):
+        out = np.zeros(self.NPARAM, np.float32)
+        self._check(self.lib.imex_mlp_get_params(self._h, _fp(out)), "get_params")
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        self._check(self.lib.imex_mlp_set_params(self._h, _fp(p)), "set_params")
+
+    def set_norm(self, x_mean, x_std, y_mean, y_std):
+        n = np.ascontiguousarray(np.concatenate([x_mean, x_std, y_mean, y_std]), np.float32)
+        self._check(self.lib.imex_mlp_set_norm(self._h, _fp(n)), "set_norm")
+
+    def norm(self):
+        n = np.zeros(2 * self.N_IN + 2 * self.N_OUT, np.float32)
+        self._check(self.lib.imex_mlp_get_norm(self._h, _fp(n)), "get_norm")
+        return n
+
+    def predict(self, x):
+        """Normalised inputs (n, 12) -> normalised outputs (n, 2)."""
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.zeros((x.shape[0], self.N_OUT), np.float32)
+        self._check(self.lib.imex_mlp_predict(self._h, _fp(x), x.shape[0], _fp(y)), "predict")
+        return y
+
+    def loss_grad(self, x, y):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        g = np.zeros(self.NPARAM, np.float32)
+        loss = C.c_float(0.0)
+        self._check(self.lib.imex_mlp_loss_grad(self._h, _fp(x), _fp(y), x.shape[0],
+                                                C.byref(loss), _fp(g)), "loss_grad")
+        return loss.value, g
+
+    def train(self, x_dev, y_dev, n, epochs=4, batch=4096, lr=1e-3, seed=7):
+        """Adam over a device-resident set (pointers to normalised float32
+        rows); returns the per-epoch mean squared error."""
+        losses = np.zeros(max(epochs, 1), np.float32)
+        self._check(self.lib.imex_mlp_train(self._h, x_dev, y_dev, int(n), int(epochs),
+                                            int(batch), float(lr), int(seed), _fp(losses)),
+                    "train")
+        return losses[:epochs]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.imex_mlp_destroy(self._h)
             self._h = None
 
     def __del__(self):
