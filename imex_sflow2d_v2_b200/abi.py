@@ -112,6 +112,7 @@ class ImexStats(C.Structure):
         ("first_error_j", C.c_int32), ("first_error_k", C.c_int32),
         ("dt", C.c_double), ("t", C.c_double),
         ("steps", C.c_int64), ("kernel_launches", C.c_int64),
+        ("warm_fallback_cells", C.c_int64),
     ]
 
 

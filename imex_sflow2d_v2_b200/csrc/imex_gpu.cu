@@ -50,6 +50,13 @@ struct ImexCtx {
   double* post_diag = nullptr;
   double* nw_buf = nullptr;      // backing store of nw's FP64 planes
   uint32_t* nw_lists = nullptr;  // backing store of nw's three cell lists
+  // learned warm start and training-pair harvest
+  struct ImexMLP* warm_mlp = nullptr;  // not owned
+  uint32_t* nw_wlist = nullptr;
+  float* nw_feat = nullptr;
+  double* nw_guess = nullptr;
+  float* h_x = nullptr;
+  float* h_y = nullptr;
   size_t scratch_bytes = 0;
   bool x_valid = false;          // X holds the fluxes of the current state
   bool exchange = false;         // erosion/deposition planes present
@@ -171,6 +178,8 @@ cudaError_t launch_flux(ImexCtx* ctx) {
   }
 }
 
+cudaError_t launch_warm_predict(ImexCtx* ctx);  // after ImexMLP (below)
+
 template <int NS>
 cudaError_t launch_stage2_ns(ImexCtx* ctx) {
   const DevParams& P = ctx->P;
@@ -184,6 +193,13 @@ cudaError_t launch_stage2_ns(ImexCtx* ctx) {
     k_stage2_first<NS><<<grid, STAGE2_THREADS, 0, ctx->stream>>>(
         ctx->dP, ctx->q, ctx->X, ctx->mask, ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy, ctx->Byy,
         ctx->gc, ctx->nw, ctx->clk);
+    if (ctx->nw.warm) {
+      cudaError_t e = launch_warm_predict(ctx);
+      if (e != cudaSuccess) return e;
+      k_stage2_wstart<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->Bx,
+                                                                     ctx->By, ctx->nw, ctx->clk);
+      ctx->launches += 1;
+    }
   }
   {
     ProfScope ps(ctx, KID_S2_ITER);
@@ -193,6 +209,16 @@ cudaError_t launch_stage2_ns(ImexCtx* ctx) {
                                                                  ctx->By, ctx->nw, ctx->clk, 3);
     k_stage2_tail<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->Bx,
                                                                  ctx->By, ctx->nw, ctx->clk);
+    if (ctx->nw.warm) {
+      k_stage2_fallback<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->Bx,
+                                                                       ctx->By, ctx->nw, ctx->clk);
+      ctx->launches += 1;
+    }
+  }
+  if (ctx->nw.harvest) {
+    k_harvest<NS><<<grid_1d(ncell, 128), 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->Bx, ctx->By,
+                                                                ctx->nw, ctx->clk);
+    ctx->launches += 1;
   }
   {
     ProfScope ps(ctx, KID_S2_POST);
@@ -592,7 +618,7 @@ int imex_gpu_destroy(ImexCtx* ctx) {
                   ctx->Byy, ctx->gc, ctx->dgc, ctx->gcsx, ctx->gcsy, ctx->release, ctx->erodible,
                   ctx->deposit, ctx->erosion, ctx->Bcent, ctx->ring, ctx->clk, ctx->scratch, ctx->dP,
                   ctx->nw_buf, ctx->nw.status, ctx->nw_lists, ctx->post_buf, ctx->post_vuln,
-                  ctx->post_diag};
+                  ctx->post_diag, ctx->nw_wlist, ctx->nw_feat, ctx->nw_guess, ctx->h_x, ctx->h_y};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (ctx->clk_host) cudaFreeHost(ctx->clk_host);
@@ -845,6 +871,7 @@ int imex_gpu_stats(ImexCtx* ctx, ImexStats* st, int reset_errors) {
   st->t = c.t;
   st->steps = c.steps;
   st->kernel_launches = ctx->launches;
+  st->warm_fallback_cells = (int64_t)c.warm_fallback;
   if (reset_errors) {
     ctx->clk_host->error_mask = 0;
     ctx->clk_host->first_error = ~0ULL;
@@ -1296,6 +1323,117 @@ int imex_mlp_train(ImexMLP* mlp, const float* x_dev, const float* y_dev, int64_t
 }
 
 const char* imex_mlp_last_error(ImexMLP* mlp) { return mlp ? mlp->last_error.c_str() : "null"; }
+
+}  // extern "C"
+
+// ============================================================ warm start
+namespace {
+template <int NS>
+cudaError_t launch_warm_predict_ns(ImexCtx* ctx) {
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_warm_predict<NS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)mlp::SMEM_NET);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  WarmNorm nrm;
+  const float* n = ctx->warm_mlp->norm;
+  for (int i = 0; i < WARM_IN; ++i) {
+    nrm.x_mean[i] = n[i];
+    nrm.x_std[i] = n[WARM_IN + i];
+  }
+  for (int i = 0; i < WARM_OUT; ++i) {
+    nrm.y_mean[i] = n[2 * WARM_IN + i];
+    nrm.y_std[i] = n[2 * WARM_IN + WARM_OUT + i];
+  }
+  k_warm_predict<NS><<<148 * 2, 32 * mlp::WARPS, mlp::SMEM_NET, ctx->stream>>>(
+      ctx->dP, ctx->nw, ctx->clk, ctx->warm_mlp->bw, ctx->warm_mlp->prm, nrm);
+  ctx->launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_warm_predict(ImexCtx* ctx) {
+  switch (ctx->ns) {
+    case 1: return launch_warm_predict_ns<1>(ctx);
+    case 2: return launch_warm_predict_ns<2>(ctx);
+    case 3: return launch_warm_predict_ns<3>(ctx);
+    default: return launch_warm_predict_ns<4>(ctx);
+  }
+}
+}  // namespace
+
+static void drop_graph(ImexCtx* ctx) {
+  if (ctx->graph_exec) { cudaGraphExecDestroy(ctx->graph_exec); ctx->graph_exec = nullptr; }
+  if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+}
+
+extern "C" {
+
+int imex_gpu_set_warmstart(ImexCtx* ctx, ImexMLP* net) {
+  if (!ctx) return IMEX_EINVAL;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (net && net->device != ctx->device)
+    return fail(ctx, IMEX_EINVAL, "imex_gpu_set_warmstart: network on another device");
+  const size_t plane = (size_t)ctx->P.plane;
+  if (net && !ctx->nw_wlist) {
+    CK(dalloc(&ctx->nw_wlist, plane * 2));   // warm-start list, then fallback list
+    CK(dalloc(&ctx->nw_feat, plane * WARM_IN));
+    CK(dalloc(&ctx->nw_guess, plane * 2));
+  }
+  ctx->warm_mlp = net;
+  ctx->nw.warm = net ? 1 : 0;
+  ctx->nw.wlist = ctx->nw_wlist;
+  ctx->nw.flist = ctx->nw_wlist ? ctx->nw_wlist + plane : nullptr;
+  ctx->nw.feat = ctx->nw_feat;
+  ctx->nw.guess = ctx->nw_guess;
+  drop_graph(ctx);
+  return IMEX_OK;
+}
+
+int imex_gpu_harvest_start(ImexCtx* ctx, int64_t capacity, int stride) {
+  if (!ctx || capacity <= 0 || stride < 1) return IMEX_EINVAL;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (ctx->h_x) cudaFree(ctx->h_x);
+  if (ctx->h_y) cudaFree(ctx->h_y);
+  ctx->h_x = nullptr;
+  ctx->h_y = nullptr;
+  CK(dalloc(&ctx->h_x, (size_t)capacity * WARM_IN));
+  CK(dalloc(&ctx->h_y, (size_t)capacity * WARM_OUT));
+  ctx->nw.harvest = 1;
+  ctx->nw.hstride = (unsigned int)stride;
+  ctx->nw.hcap = (unsigned long long)capacity;
+  ctx->nw.hx = ctx->h_x;
+  ctx->nw.hy = ctx->h_y;
+  const unsigned long long zero = 0;
+  CK(cudaMemcpy(&ctx->clk->harvest_n, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+  drop_graph(ctx);
+  return IMEX_OK;
+}
+
+int imex_gpu_harvest_stop(ImexCtx* ctx) {
+  if (!ctx) return IMEX_EINVAL;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->nw.harvest = 0;
+  drop_graph(ctx);
+  return IMEX_OK;
+}
+
+int imex_gpu_harvest_data(ImexCtx* ctx, const float** x_dev, const float** y_dev, int64_t* n) {
+  if (!ctx || !n) return IMEX_EINVAL;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  unsigned long long cnt = 0;
+  CK(cudaMemcpy(&cnt, &ctx->clk->harvest_n, sizeof(cnt), cudaMemcpyDeviceToHost));
+  *n = (int64_t)std::min<unsigned long long>(cnt, ctx->nw.hcap);
+  if (x_dev) *x_dev = ctx->h_x;
+  if (y_dev) *y_dev = ctx->h_y;
+  return IMEX_OK;
+}
 
 }  // extern "C"
 

@@ -19,6 +19,7 @@
 #pragma once
 
 #include "imex_device.cuh"
+#include "imex_mlp.cuh"
 
 namespace imex {
 
@@ -55,6 +56,11 @@ struct DevClock {
   unsigned long long solve_cells;
   unsigned long long steps;
   unsigned int nw_count[4];  // cells appended to the stage-2 Newton lists
+                             // ([3]: the warm-start list)
+  unsigned long long harvest_n;      // training pairs written so far
+  unsigned long long warm_fallback;  // warm starts redone from q_si
+  unsigned int nw_fb;                // cells in the warm-start fallback list
+  int pad2_;
 };
 
 IMEX_HD double x_stag(const DevParams& P, int J) { return P.x0 + (double)(J - 1) * P.dx; }
@@ -1044,20 +1050,68 @@ struct NewtonWork {
   uint8_t* status;  // 1 plane: bit 0 the cell went through Newton, bit 1 its
                     // residual must be evaluated again (see newton_iterk)
   uint32_t* list[3];  // cells (k*pitch + j) still iterating after pass 0, 1, 2
+  // learned warm start (warm != 0): the Newton cells of the step, their
+  // network inputs and the network's momentum guesses
+  int warm;
+  uint32_t* wlist;    // Newton cells, in append order
+  uint32_t* flist;    // warm starts to redo from q_si (k_stage2_fallback)
+  float* feat;        // WARM_IN floats per wlist entry
+  double* guess;      // 2 planes: proposed q(2), q(3)
+  // training pairs (harvest != 0): inputs and targets of every `stride`-th
+  // Newton cell, up to `cap` pairs
+  int harvest;
+  unsigned int hstride;
+  unsigned long long hcap;
+  float* hx;
+  float* hy;
+};
+
+// Network inputs of one Newton cell: class-count independent quantities of
+// q_si, the old state, the explicit tendency, dt and the slope.  Targets:
+// the change of the two momentum components over the Newton solve, per unit
+// of q(1).
+constexpr int WARM_IN = 12, WARM_OUT = 2;
+
+template <int NS>
+__device__ __forceinline__ void warm_features(const double* qsi, const double* q0,
+                                              const double* Rj, double dt, double bx,
+                                              double by, float* f) {
+  const double m = qsi[0], im = 1.0 / m;
+  double xs = 0.0;
+#pragma unroll
+  for (int i = 0; i < NS; ++i) xs += qsi[4 + i];
+  f[0] = (float)log10(fmax(m, 1.0e-12));
+  f[1] = (float)(qsi[1] * im);
+  f[2] = (float)(qsi[2] * im);
+  f[3] = (float)(q0[1] * im);
+  f[4] = (float)(q0[2] * im);
+  f[5] = (float)(dt * Rj[1] * im);
+  f[6] = (float)(dt * Rj[2] * im);
+  f[7] = (float)(qsi[3] * im * 1.0e-6);
+  f[8] = (float)(xs * im);
+  f[9] = (float)log10(dt);
+  f[10] = (float)bx;
+  f[11] = (float)by;
+}
+
+struct WarmNorm {
+  float x_mean[WARM_IN], x_std[WARM_IN], y_mean[WARM_OUT], y_std[WARM_OUT];
 };
 
 constexpr int STAGE2_THREADS = 128;
 
-__device__ __forceinline__ void list_append(bool add, uint32_t c, uint32_t* list,
-                                            unsigned int* count) {
+__device__ __forceinline__ unsigned int list_append(bool add, uint32_t c, uint32_t* list,
+                                                    unsigned int* count) {
   const unsigned m = __ballot_sync(0xffffffffu, add);
-  if (!m) return;
+  if (!m) return 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int leader = __ffs(m) - 1;
   unsigned int base = 0;
   if (lane == leader) base = atomicAdd(count, (unsigned int)__popc(m));
   base = __shfl_sync(0xffffffffu, base, leader);
-  if (add) list[base + __popc(m & ((1u << lane) - 1u))] = c;
+  const unsigned int slot = base + __popc(m & ((1u << lane) - 1u));
+  if (add) list[slot] = c;
+  return add ? slot : 0xffffffffu;
 }
 
 // Newton statistics of the cells that finished in this warp iteration
@@ -1094,6 +1148,41 @@ __device__ __forceinline__ void newton_flush_stats(DevClock* clk, unsigned long 
 }
 
 template <int NS>
+__device__ __forceinline__ bool all_finite(const double* v) {
+  bool ok = true;
+#pragma unroll
+  for (int i = 0; i < 4 + NS; ++i) ok &= isfinite(v[i]);
+  return ok;
+}
+
+// Fallback of a warm start that failed (no convergence in 100 iterations, or
+// a non-finite result): the plain solve_rk_step from q_si.  Returns its
+// iteration count; qj receives its result.  Run by k_stage2_fallback only.
+template <int NS>
+__device__ __forceinline__ int newton_plain(const DevParams& P, const NewtonWork& W, size_t c,
+                                         const double* q0, const double* Rj, double bx,
+                                         double by, double dt, double* qj,
+                                         unsigned long long& trials) {
+  constexpr int NV = 4 + NS;
+  const size_t N = (size_t)P.plane;
+  double qj_org[NV], qj_rel[NV], rt[NV], scal_f;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) qj[i] = W.qsi[c + i * N];
+  newton_scale<NS>(qj, qj_org);
+  if (newton_start<NS>(P, qj, q0, Rj, bx, by, dt, qj_org, qj_rel, rt, scal_f)) return 1;
+  if (newton_iter1<NS>(P, qj, q0, Rj, bx, by, dt, qj_org, qj_rel, rt, scal_f)) return 1;
+  bool stale = false;
+  int it;
+  for (it = 2; it <= NEWTON_MAX_IT; ++it) {
+    long long tr = 0;
+    bool done = newton_iterk<NS>(P, qj, q0, Rj, bx, by, dt, qj_org, qj_rel, rt, scal_f, tr, stale);
+    trials += (unsigned long long)tr;
+    if (done) break;
+  }
+  return it > NEWTON_MAX_IT ? NEWTON_MAX_IT : it;
+}
+
+template <int NS>
 __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
     k_stage2_first(const DevParams* __restrict__ Pp, const double* __restrict__ q,
                    const double* __restrict__ X, const uint8_t* __restrict__ mask,
@@ -1113,8 +1202,9 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
        base += stride) {
     const long long g = base + (threadIdx.x & 31);
     size_t c = 0;
-    bool go_on = false;
+    bool go_on = false, warm_cell = false;
     int fin = 0;
+    float fw[WARM_IN];
     if (g < ncell) {
       const int j = (int)(g % nx), k = (int)(g / nx);
       c = (size_t)k * P.pitch + j;
@@ -1177,6 +1267,11 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
           W.status[c] = 1;
           cells += 1;
           double qj_org[NV], qj_rel[NV], rt[NV], scal_f;
+          if (W.warm) {
+            // Newton waits for the network's guess (k_warm_predict, k_stage2_wstart)
+            warm_features<NS>(qsi, q0, Rj, dt, bx, by, fw);
+            warm_cell = true;
+          } else {
           newton_scale<NS>(qg, qj_org);
           if (newton_start<NS>(P, qg, q0, Rj, bx, by, dt, qj_org, qj_rel, rt, scal_f)) {
             fin = 1;
@@ -1191,12 +1286,13 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
             }
             W.sf[c] = scal_f;
           }
+          }
         } else {
 #pragma unroll
           for (int i = 0; i < NV; ++i) qg[i] = qfv[i];
           W.status[c] = 0;
         }
-        if (!go_on) {
+        if (!go_on && !warm_cell) {
 #pragma unroll
           for (int i = 0; i < NV; ++i) W.x[c + i * N] = qg[i];
         }
@@ -1204,6 +1300,13 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
     }
     newton_finish_stats(clk, fin, it_sum, maxit);
     list_append(go_on, (uint32_t)c, W.list[0], &clk->nw_count[0]);
+    if (W.warm) {
+      const unsigned int slot = list_append(warm_cell, (uint32_t)c, W.wlist, &clk->nw_count[3]);
+      if (warm_cell) {
+#pragma unroll
+        for (int i = 0; i < WARM_IN; ++i) W.feat[(size_t)slot * WARM_IN + i] = fw[i];
+      }
+    }
   }
   newton_flush_stats(clk, cells, it_sum, 0, maxit);
 }
@@ -1227,7 +1330,7 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
        base += stride) {
     const long long e = base + (threadIdx.x & 31);
     uint32_t c = 0;
-    bool go_on = false;
+    bool go_on = false, fb = false;
     int fin = 0;
     if (e < n) {
       c = in[e];
@@ -1240,6 +1343,10 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
         qj_rel[i] = W.x[c + i * N];
         rt[i] = W.rt[c + i * N];
       }
+      if (W.warm) {   // the Newton start (scaling source) was the network's guess
+        qj[1] = W.guess[c];
+        qj[2] = W.guess[c + N];
+      }
       scal_f = W.sf[c];
       bool stale = (W.status[c] & 2) != 0;
       newton_scale<NS>(qj, qj_org);
@@ -1249,8 +1356,12 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
       trials += (unsigned long long)tr;
       if (done || nl_iter >= NEWTON_MAX_IT) {
         fin = nl_iter;
+        if (W.warm && (!done || !all_finite<NS>(qj))) {
+          fb = true;
+        } else {
 #pragma unroll
-        for (int i = 0; i < NV; ++i) W.x[c + i * N] = qj[i];
+          for (int i = 0; i < NV; ++i) W.x[c + i * N] = qj[i];
+        }
       } else {
         go_on = true;
 #pragma unroll
@@ -1264,6 +1375,7 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
     }
     newton_finish_stats(clk, fin, it_sum, maxit);
     list_append(go_on, c, out, &clk->nw_count[nl_iter - 1]);
+    if (W.warm) list_append(fb, c, W.flist, &clk->nw_fb);
   }
   newton_flush_stats(clk, 0, it_sum, trials, maxit);
 }
@@ -1285,8 +1397,10 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
        base += stride) {
     const long long e = base + (threadIdx.x & 31);
     int fin = 0;
+    bool fb = false;
+    uint32_t c = 0;
     if (e < n) {
-      const uint32_t c = W.list[2][e];
+      c = W.list[2][e];
       double q0[NV], Rj[NV], qj_org[NV], qj_rel[NV], rt[NV], qj[NV], scal_f;
 #pragma unroll
       for (int i = 0; i < NV; ++i) {
@@ -1295,6 +1409,10 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
         qj[i] = W.qsi[c + i * N];
         qj_rel[i] = W.x[c + i * N];
         rt[i] = W.rt[c + i * N];
+      }
+      if (W.warm) {
+        qj[1] = W.guess[c];
+        qj[2] = W.guess[c + N];
       }
       scal_f = W.sf[c];
       bool stale = (W.status[c] & 2) != 0;
@@ -1309,12 +1427,210 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
         if (done) break;
       }
       fin = it > NEWTON_MAX_IT ? NEWTON_MAX_IT : it;
+      if (W.warm && (it > NEWTON_MAX_IT || !all_finite<NS>(qj))) {
+        fb = true;
+      } else {
 #pragma unroll
-      for (int i = 0; i < NV; ++i) W.x[c + i * N] = qj[i];
+        for (int i = 0; i < NV; ++i) W.x[c + i * N] = qj[i];
+      }
     }
     newton_finish_stats(clk, fin, it_sum, maxit);
+    if (W.warm) list_append(fb, c, W.flist, &clk->nw_fb);
   }
   newton_flush_stats(clk, 0, it_sum, trials, maxit);
+}
+
+// The network's momentum guesses for the cells of the warm-start list:
+// 16 cells per warp through the tensor-core forward pass.
+template <int NS>
+__global__ void __launch_bounds__(32 * mlp::WARPS)
+    k_warm_predict(const DevParams* __restrict__ Pp, NewtonWork W, DevClock* clk,
+                   const __nv_bfloat16* __restrict__ gW, const float* __restrict__ gP,
+                   WarmNorm nrm) {
+  const DevParams& P = *Pp;
+  const size_t N = (size_t)P.plane;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __nv_bfloat16* sW = reinterpret_cast<__nv_bfloat16*>(smem);
+  float* sP = reinterpret_cast<float*>(smem + mlp::NBW * sizeof(__nv_bfloat16));
+  __shared__ float xin[mlp::WARPS][16 * WARM_IN];
+  __shared__ float yout[mlp::WARPS][16 * WARM_OUT];
+  mlp::load_net(gW, gP, sW, sP);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long n = (long long)clk->nw_count[3];
+  for (long long r0 = ((long long)blockIdx.x * mlp::WARPS + warp) * 16; r0 < n;
+       r0 += (long long)gridDim.x * mlp::WARPS * 16) {
+    const int nv = (int)((n - r0) < 16 ? (n - r0) : 16);
+    for (int e = lane; e < 16 * WARM_IN; e += 32) {
+      const int r = e / WARM_IN, k = e % WARM_IN;
+      xin[warp][e] = r < nv ? (W.feat[(size_t)(r0 + r) * WARM_IN + k] - nrm.x_mean[k]) / nrm.x_std[k]
+                            : 0.0f;
+    }
+    __syncwarp();
+    mlp::forward16(xin[warp], nv, sW, sP, yout[warp], WARM_OUT, nullptr);
+    __syncwarp();
+    if (lane < nv) {
+      const uint32_t c = W.wlist[r0 + lane];
+      const double m = W.qsi[c];
+#pragma unroll
+      for (int k = 0; k < WARM_OUT; ++k) {
+        const double tk = (double)yout[warp][lane * WARM_OUT + k] * nrm.y_std[k] + nrm.y_mean[k];
+        W.guess[c + k * N] = W.qsi[c + (1 + k) * N] + m * tk;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// Newton scaling and iteration 1 from the network's guess for the cells of
+// the warm-start list; cells still iterating go to list 0 as in
+// k_stage2_first.
+template <int NS>
+__global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
+    k_stage2_wstart(const DevParams* __restrict__ Pp, const double* __restrict__ q,
+                    const double* __restrict__ Bx, const double* __restrict__ By, NewtonWork W,
+                    DevClock* clk) {
+  const DevParams& P = *Pp;
+  constexpr int NV = 4 + NS;
+  const size_t N = (size_t)P.plane;
+  const double dt = clk->dt;
+  const long long n = (long long)clk->nw_count[3];
+  unsigned long long it_sum = 0, maxit = 0, trials = 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n;
+       base += stride) {
+    const long long e = base + (threadIdx.x & 31);
+    uint32_t c = 0;
+    bool go_on = false, fb = false;
+    int fin = 0;
+    if (e < n) {
+      c = W.wlist[e];
+      double q0[NV], Rj[NV], qj[NV], qj_org[NV], qj_rel[NV], rt[NV], scal_f;
+#pragma unroll
+      for (int i = 0; i < NV; ++i) {
+        q0[i] = q[c + i * N];
+        Rj[i] = W.Rj[c + i * N];
+        qj[i] = W.qsi[c + i * N];
+      }
+      qj[1] = W.guess[c];
+      qj[2] = W.guess[c + N];
+      const double bx = Bx[c], by = By[c];
+      newton_scale<NS>(qj, qj_org);
+      bool done = newton_start<NS>(P, qj, q0, Rj, bx, by, dt, qj_org, qj_rel, rt, scal_f) ||
+                  newton_iter1<NS>(P, qj, q0, Rj, bx, by, dt, qj_org, qj_rel, rt, scal_f);
+      if (done) {
+        fin = 1;
+        if (!all_finite<NS>(qj)) {
+          fb = true;
+        } else {
+#pragma unroll
+          for (int i = 0; i < NV; ++i) W.x[c + i * N] = qj[i];
+        }
+      } else {
+        go_on = true;
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+          W.x[c + i * N] = qj_rel[i];
+          W.rt[c + i * N] = rt[i];
+        }
+        W.sf[c] = scal_f;
+      }
+    }
+    newton_finish_stats(clk, fin, it_sum, maxit);
+    list_append(go_on, c, W.list[0], &clk->nw_count[0]);
+    list_append(fb, c, W.flist, &clk->nw_fb);
+  }
+  newton_flush_stats(clk, 0, it_sum, trials, maxit);
+}
+
+// Warm starts that failed, redone with the plain start (q_si).
+template <int NS>
+__global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
+    k_stage2_fallback(const DevParams* __restrict__ Pp, const double* __restrict__ q,
+                      const double* __restrict__ Bx, const double* __restrict__ By,
+                      NewtonWork W, DevClock* clk) {
+  const DevParams& P = *Pp;
+  constexpr int NV = 4 + NS;
+  const size_t N = (size_t)P.plane;
+  const double dt = clk->dt;
+  const long long n = (long long)clk->nw_fb;
+  unsigned long long it_sum = 0, trials = 0;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const uint32_t c = W.flist[e];
+    double q0[NV], Rj[NV], qj[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      q0[i] = q[c + i * N];
+      Rj[i] = W.Rj[c + i * N];
+    }
+    it_sum += (unsigned long long)newton_plain<NS>(P, W, c, q0, Rj, Bx[c], By[c], dt, qj, trials);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) W.x[c + i * N] = qj[i];
+    atomicAdd(&clk->warm_fallback, 1ULL);
+  }
+  if (it_sum) atomicAdd(&clk->newton_iters, it_sum);
+  if (trials) atomicAdd(&clk->lnsrch_trials, trials);
+}
+
+// Training pairs from the finished Newton solves (before the sign guard):
+// the inputs of warm_features and the momentum change per unit q(1), for
+// every hstride-th Newton cell (cells taken by a hash of their index and
+// the step, so that successive steps sample different cells).
+template <int NS>
+__global__ void __launch_bounds__(128)
+    k_harvest(const DevParams* __restrict__ Pp, const double* __restrict__ q,
+              const double* __restrict__ Bx, const double* __restrict__ By, NewtonWork W,
+              DevClock* clk) {
+  const DevParams& P = *Pp;
+  constexpr int NV = 4 + NS;
+  const int nx = P.nx;
+  const long long ncell = (long long)nx * P.ny;
+  const size_t N = (size_t)P.plane;
+  const double dt = clk->dt;
+  const unsigned long long salt = clk->steps * 0x9E3779B97F4A7C15ULL;
+  for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < ncell;
+       base += (long long)gridDim.x * blockDim.x) {
+    const long long g = base + (threadIdx.x & 31);
+    bool take = false;
+    size_t c = 0;
+    float f[WARM_IN], y[WARM_OUT];
+    if (g < ncell) {
+      c = (size_t)(g / nx) * P.pitch + (size_t)(g % nx);
+      unsigned long long h = ((unsigned long long)g + salt) * 0xBF58476D1CE4E5B9ULL;
+      h ^= h >> 31;
+      if ((W.status[c] & 1) && (h % W.hstride) == 0) {
+        double q0[NV], qsi[NV], Rj[NV], x1, x2;
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+          q0[i] = q[c + i * N];
+          qsi[i] = W.qsi[c + i * N];
+          Rj[i] = W.Rj[c + i * N];
+        }
+        x1 = W.x[c + N];
+        x2 = W.x[c + 2 * N];
+        if (qsi[0] > 0.0 && isfinite(x1) && isfinite(x2)) {
+          warm_features<NS>(qsi, q0, Rj, dt, Bx[c], By[c], f);
+          y[0] = (float)((x1 - qsi[1]) / qsi[0]);
+          y[1] = (float)((x2 - qsi[2]) / qsi[0]);
+          take = true;
+        }
+      }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, take);
+    if (!m) continue;
+    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    unsigned long long slot0 = 0;
+    if (lane == leader) slot0 = atomicAdd(&clk->harvest_n, (unsigned long long)__popc(m));
+    slot0 = __shfl_sync(0xffffffffu, slot0, leader);
+    const unsigned long long slot = slot0 + __popc(m & ((1u << lane) - 1u));
+    if (take && slot < W.hcap) {
+#pragma unroll
+      for (int i = 0; i < WARM_IN; ++i) W.hx[slot * WARM_IN + i] = f[i];
+      W.hy[slot * WARM_OUT + 0] = y[0];
+      W.hy[slot * WARM_OUT + 1] = y[1];
+    }
+  }
 }
 
 // Sign guard after Newton (src/solver_2d.f90:1238-1255) and assemble_sol
@@ -1472,12 +1788,14 @@ __global__ void k_step_begin(DevClock* clk, double max_dt, int reset_cells) {
   clk->newton_iters = 0;
   clk->lnsrch_trials = 0;
   clk->newton_maxit = 0;
+  clk->warm_fallback = 0;
   for (int b = 0; b < 16; ++b) clk->hist[b] = 0;
 }
 
 // Empties the stage-2 Newton lists (before each stage 2).
 __global__ void k_nw_reset(DevClock* clk) {
   for (int i = 0; i < 4; ++i) clk->nw_count[i] = 0;
+  clk->nw_fb = 0;
 }
 
 // dt from the CFL minimum with the driver's clipping (src/IMEX_SfloW2D.f90:359-381).

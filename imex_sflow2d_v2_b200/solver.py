@@ -82,6 +82,10 @@ def load_library(path=LIB_PATH):
         "imex_mlp_train": ([vp, vp, vp, C.c_int64, C.c_int, C.c_int, C.c_float, C.c_uint64,
                             C.POINTER(C.c_float)], C.c_int),
         "imex_mlp_last_error": ([vp], C.c_char_p),
+        "imex_gpu_set_warmstart": ([vp, vp], C.c_int),
+        "imex_gpu_harvest_start": ([vp, C.c_int64, C.c_int], C.c_int),
+        "imex_gpu_harvest_stop": ([vp], C.c_int),
+        "imex_gpu_harvest_data": ([vp, C.POINTER(vp), C.POINTER(vp), i64p], C.c_int),
         "imex_gpu_ensemble_create": ([C.c_int, C.POINTER(C.POINTER(ImexParams)),
                                       C.POINTER(C.POINTER(ImexStatic)), C.c_int,
                                       C.POINTER(vp)], C.c_int),
@@ -236,6 +240,28 @@ class ImexSolver:
                                                C.byref(nt)), "get_post")
         f = [x.reshape((self.nx, self.ny), order="F") for x in a]
         return f[0], f[1], f[2], v[:nt.value * n].reshape((nt.value, self.nx, self.ny), order="F")
+
+    # -- learned Newton warm start
+    def set_warmstart(self, net):
+        """Start stage 2's Newton solves from `net`'s guess (an ImexMLP), or
+        from q_si again with None."""
+        return self._check(self.lib.imex_gpu_set_warmstart(self._h, net._h if net else None),
+                           "set_warmstart")
+
+    def harvest_start(self, capacity, stride=1):
+        return self._check(self.lib.imex_gpu_harvest_start(self._h, int(capacity), int(stride)),
+                           "harvest_start")
+
+    def harvest_stop(self):
+        return self._check(self.lib.imex_gpu_harvest_stop(self._h), "harvest_stop")
+
+    def harvest_data(self):
+        """(x device pointer, y device pointer, pairs): float32 rows of 12 and 2."""
+        x, y = C.c_void_p(), C.c_void_p()
+        n = C.c_int64(0)
+        self._check(self.lib.imex_gpu_harvest_data(self._h, C.byref(x), C.byref(y), C.byref(n)),
+                    "harvest_data")
+        return x.value, y.value, n.value
 
     def timestep_noalloc(self):
         """CFL dt like timestep(), through the entry point that allocates

@@ -166,6 +166,7 @@ typedef struct ImexStats {
   double t;                        /* model time held by the context */
   int64_t steps;                   /* steps taken through imex_gpu_advance */
   int64_t kernel_launches;         /* kernels launched by the context since create */
+  int64_t warm_fallback_cells;     /* warm starts redone from q_si in the last step */
 } ImexStats;
 
 typedef struct ImexCtx ImexCtx;
@@ -276,6 +277,44 @@ int imex_gpu_post_step(ImexCtx* ctx, ImexPostDiag* diag /* NULL: no print values
 int imex_gpu_post_diag(ImexCtx* ctx, ImexPostDiag* diag);
 int imex_gpu_get_post(ImexCtx* ctx, double* hmax, double* pdynmax, double* mod_vel_max,
                       int8_t* vuln_table, int* n_table);
+
+/*
+ * Learned Newton warm start (no counterpart in the reference).  A small
+ * network (12 inputs -> 3 x 64 SiLU -> 2 outputs; BF16 weights on tensor
+ * cores, FP32 accumulation) proposes the two momentum components that stage
+ * 2's Newton solve (src/solver_2d.f90:1660-1994) starts from; the solve then
+ * runs in FP64 to the reference's own exit tests, its scaling taken from the
+ * proposed start.  A start that does not converge in 100 iterations or ends
+ * non-finite is redone from q_si (the plain start); ImexStats counts those.
+ * Results equal the plain method's to the solver's tolerance, not bit for
+ * bit.  Training pairs come from the solver itself: imex_gpu_harvest_start
+ * records, for every stride-th Newton cell of each following stage 2, the 12
+ * inputs and the converged momentum change per unit q(1), up to `capacity`
+ * pairs, into device buffers that imex_gpu_harvest_data exposes (valid until
+ * the next harvest_start or destroy).  The network is trained on them with
+ * imex_mlp_train (own forward/backward/Adam kernels) and attached with
+ * imex_gpu_set_warmstart (NULL returns to the plain start; the network must
+ * outlive its use).  Inputs and targets are normalised by imex_mlp_set_norm
+ * (x mean[12], x std[12], y mean[2], y std[2]).
+ */
+typedef struct ImexMLP ImexMLP;
+#define IMEX_MLP_NPARAM 9928
+int imex_mlp_create(int device, uint64_t seed, ImexMLP** out);
+int imex_mlp_destroy(ImexMLP* net);
+int imex_mlp_get_params(ImexMLP* net, float* params /* IMEX_MLP_NPARAM */);
+int imex_mlp_set_params(ImexMLP* net, const float* params);
+int imex_mlp_set_norm(ImexMLP* net, const float* norm /* 28 floats */);
+int imex_mlp_get_norm(ImexMLP* net, float* norm);
+int imex_mlp_predict(ImexMLP* net, const float* x /* (n,12) */, int64_t n, float* y /* (n,2) */);
+int imex_mlp_loss_grad(ImexMLP* net, const float* x, const float* y, int64_t n, float* loss,
+                       float* grad /* IMEX_MLP_NPARAM */);
+int imex_mlp_train(ImexMLP* net, const float* x_dev, const float* y_dev, int64_t n, int epochs,
+                   int batch, float lr, uint64_t seed, float* loss_per_epoch);
+const char* imex_mlp_last_error(ImexMLP* net);
+int imex_gpu_set_warmstart(ImexCtx* ctx, ImexMLP* net);
+int imex_gpu_harvest_start(ImexCtx* ctx, int64_t capacity, int stride);
+int imex_gpu_harvest_stop(ImexCtx* ctx);
+int imex_gpu_harvest_data(ImexCtx* ctx, const float** x_dev, const float** y_dev, int64_t* n);
 
 /*
  * Ensembles: many independent runs (members), each with its own grid,
