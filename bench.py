@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--ens-members", type=int, default=256)
     ap.add_argument("--ens-steps", type=int, default=1000)
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--learned-pairs", type=int, default=10_000_000)
+    ap.add_argument("--learned-n", type=int, default=1024, help="side of the comparison grid")
     return ap.parse_args()
 
 
@@ -212,6 +215,69 @@ def run_ensemble(args):
                     "d logU[1e-5,1e-3] m)"}
 
 
+def run_learned(args, g, p):
+    """Learned vs plain Newton start (fifth workload): pairs harvested from the
+    benchmark's own 4096^2 fractal run (third workload), the network trained
+    on them by the library's kernels, then the radial-current workload (1024^2,
+    two solid classes, Voellmy) stepped from one state with the plain start
+    and with the learned one."""
+    import numpy as np
+    from imex_sflow2d_v2_b200 import configs, warmstart
+    from imex_sflow2d_v2_b200.solver import ImexMLP, ImexSolver
+    cells = p.nx * p.ny
+    stride = max(1, int(cells // max(1, args.learned_pairs // 5)))
+    g.harvest_start(capacity=args.learned_pairs, stride=stride)
+    hsteps = 0
+    while g.harvest_data()[2] < args.learned_pairs and hsteps < 40:
+        g.advance(1)
+        hsteps += 1
+    g.harvest_stop()
+    net = ImexMLP(seed=20261203)
+    t0 = time.perf_counter()
+    n_pairs, losses = warmstart.train(net, g, epochs=3, batch=8192, lr=2e-3)
+    train_s = time.perf_counter() - t0
+    # comparison workload: develop the current, then the same steps both ways
+    pr, str_, qr = configs.radial_current(nx=args.learned_n, ny=args.learned_n)
+    d = ImexSolver(pr, str_)
+    d.set_state(qr, 0.0)
+    d.set_clock(0.0, 1e-2)
+    d.advance(300)
+    q_dev, t_dev = d.get_state(), d.stats().t
+    d.close()
+    out = {}
+    states = {}
+    for mode in ("plain", "learned"):
+        r = ImexSolver(pr, str_)
+        r.set_state(q_dev, t_dev)
+        r.set_clock(t_dev, 1e-2)
+        if mode == "learned":
+            r.set_warmstart(net)
+        r.profile(True)
+        its = cellsn = fb = 0
+        steps = 20
+        for _ in range(steps):
+            r.advance(1)
+            st_ = r.stats()
+            its += st_.newton_iters
+            cellsn += st_.newton_cells
+            fb += st_.warm_fallback_cells
+        kt = r.kernel_times()
+        s2 = sum(kt[k][0] for k in ("stage2_first", "stage2_iter", "stage2_post")) / steps
+        states[mode] = r.get_state()
+        out[mode] = {"newton_iters_per_cell": its / max(1, cellsn), "newton_cells": cellsn,
+                     "stage2_ms_per_step": s2, "fallback_cells": fb}
+        r.close()
+    a, b = states["plain"], states["learned"]
+    diff = float(np.abs(a - b).sum() / max(np.abs(a).sum(), 1e-300))
+    net.close()
+    return {"train_pairs": n_pairs, "harvest_steps": hsteps, "harvest_stride": stride,
+            "train_epochs": len(losses), "train_loss_per_epoch": [float(x) for x in losses],
+            "train_seconds": train_s, "compare_workload": "radial current %d^2, 2 solid classes, "
+            "Voellmy; 300 plain steps, then 20 steps each way" % args.learned_n,
+            "plain": out["plain"], "learned": out["learned"],
+            "rel_l1_learned_vs_plain_after_20_steps": diff}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -357,6 +423,9 @@ def main():
                "h2d_bytes_per_step": nv * cells * 8, "d2h_bytes_per_step": nv * cells * 8,
                "steps": args.e2e_steps}
 
+    learned = None
+    if rank == 0 and world == 1 and not args.no_learned:
+        learned = run_learned(args, g, p)
     g.close()
     ensemble = None
     if rank == 0 and world == 1 and not args.no_ensemble:
@@ -391,6 +460,7 @@ def main():
             "cpu_baseline": cb,
             "errors": int(s1.error_mask),
             "ensemble": ensemble,
+            "learned_vs_plain": learned,
         }
         print(json.dumps(line), flush=True)
     g.close()
