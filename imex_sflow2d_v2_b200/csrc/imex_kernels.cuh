@@ -294,11 +294,67 @@ IMEX_FLAT void cell_faces(const DevParams& P, const Tile<NS>& T, int lx, int ly,
 
 // One interface: left/lower state from cell a, right/upper from cell b.
 // Writes the KT flux H (n_vars) and max(|a+|,|a-|) for the CFL.
+// Limited MUSCL increments of one direction, precomputed once per cell for
+// the cells whose faces need none of cell_faces' special rules: not on the
+// domain border in that direction, not an inlet cell, no inlet-interior
+// neighbour in that direction (so the stage and timestep views agree).
+// There the faces are qp -/+ rc_d*limit(...) for every variable, exactly the
+// operations of cell_faces.  Indexed [ly - 1][lx - 1] of the shared tile:
+// x faces use rows 2..9 and columns 1..34, y faces rows 1..10, columns 2..33.
+template <int NS>
+struct SlopeTile {
+  double dq[6 + NS][TY + 2][TX + 2];
+  uint8_t ok[TY + 2][TX + 2];
+};
+
+template <int NS>
+__device__ __forceinline__ void precompute_slopes(const DevParams& P, const Tile<NS>& T,
+                                                  SlopeTile<NS>& D, int dir, int j0, int k0,
+                                                  const uint8_t* __restrict__ mask) {
+  constexpr int NP = 6 + NS;
+  const int nx = P.nx, ny = P.ny;
+  const bool rad = P.radial_source_flag != 0;
+  const int rw = (dir == 1) ? TX + 2 : TX, rh = (dir == 1) ? TY : TY + 2;
+  for (int e = threadIdx.x; e < rw * rh; e += blockDim.x) {
+    const int lx = (dir == 1) ? 1 + e % rw : HALO + e % rw;
+    const int ly = (dir == 1) ? HALO + e / rw : 1 + e / rw;
+    const int j = j0 + lx - HALO, k = k0 + ly - HALO;
+    uint8_t ok = 0;
+    const int I = (dir == 1) ? j + 1 : k + 1, n = (dir == 1) ? nx : ny;
+    if (j >= 0 && j < nx && k >= 0 && k < ny && I > 1 && I < n) {
+      const uint8_t inf = T.info[ly][lx];
+      const int dx_ = (dir == 1) ? 1 : 0, dy_ = (dir == 1) ? 0 : 1;
+      // an active interface on either side: the cell or a neighbour is solved
+      const bool used = (inf & 128) || (T.info[ly - dy_][lx - dx_] & 128) ||
+                        (T.info[ly + dy_][lx + dx_] & 128);
+      const bool plain = !(rad && (inf & CI_SRC_MASK) != 0) &&
+                         !(rad && (T.info[ly - dy_][lx - dx_] & CI_SRC_MASK) == 1) &&
+                         !(rad && (T.info[ly + dy_][lx + dx_] & CI_SRC_MASK) == 1);
+      if (used && plain) {
+        const double dh = (dir == 1) ? P.dx2 : P.dy2;
+        const double rc_d = P.reconstr_coeff * dh;
+        const double z1 = (dir == 1) ? x_comp(P, I - 1) : y_comp(P, I - 1);
+        const double z2 = (dir == 1) ? x_comp(P, I) : y_comp(P, I);
+        const double z3 = (dir == 1) ? x_comp(P, I + 1) : y_comp(P, I + 1);
+#pragma unroll 1
+        for (int i = 0; i < NP; ++i) {
+          const double v1 = T.qp[i][ly - dy_][lx - dx_], v2 = T.qp[i][ly][lx],
+                       v3 = T.qp[i][ly + dy_][lx + dx_];
+          D.dq[i][ly - 1][lx - 1] = rc_d * limit(v1, v2, v3, z1, z2, z3, P.limiter[i], P.theta);
+        }
+        ok = 1;
+      }
+    }
+    D.ok[ly - 1][lx - 1] = ok;
+  }
+}
+
 template <int NS>
 IMEX_FLAT void interface_flux(const DevParams& P, const Tile<NS>& T, int dir, int la_x,
                                int la_y, int ja, int ka, bool a_in, bool b_in, double gcf,
                                bool stage, double time, const RingCell* ring, double* H,
-                               double& amax_flux, double& aneg_out, double& apos_out) {
+                               double& amax_flux, double& aneg_out, double& apos_out,
+                               const SlopeTile<NS>* D = nullptr) {
   constexpr int NV = 4 + NS, NP = 6 + NS;
   const int lb_x = (dir == 1) ? la_x + 1 : la_x, lb_y = (dir == 1) ? la_y : la_y + 1;
   const int jb = (dir == 1) ? ja + 1 : ja, kb = (dir == 1) ? ka : ka + 1;
@@ -315,8 +371,18 @@ IMEX_FLAT void interface_flux(const DevParams& P, const Tile<NS>& T, int dir, in
 #pragma unroll 1
   for (int side = 0; side < 2; ++side) {
     if (!(side == 0 ? comp_a : comp_b)) continue;
-    cell_faces<NS>(P, T, side ? lb_x : la_x, side ? lb_y : la_y, side ? jb : ja, side ? kb : ka,
-                   dir, stage, time, ring, tmpm, tmpp);
+    const int sx = side ? lb_x : la_x, sy = side ? lb_y : la_y;
+    if (D && stage && D->ok[sy - 1][sx - 1]) {
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        const double v2 = T.qp[i][sy][sx], dq = D->dq[i][sy - 1][sx - 1];
+        tmpm[i] = v2 - dq;
+        tmpp[i] = v2 + dq;
+      }
+    } else {
+      cell_faces<NS>(P, T, sx, sy, side ? jb : ja, side ? kb : ka, dir, stage, time, ring,
+                     tmpm, tmpp);
+    }
 #pragma unroll
     for (int i = 0; i < NP; ++i) {
       if (side == 0) QL[i] = tmpp[i];   // a's plus face
@@ -407,6 +473,7 @@ IMEX_FLAT void interface_flux(const DevParams& P, const Tile<NS>& T, int dir, in
 template <int NS>
 struct FluxShared {
   Tile<NS> tile;
+  SlopeTile<NS> slopes;
   double Hx[4 + NS][TY][TX + 1];
   double Hy[4 + NS][TY + 1][TX];
   double ax[TY][TX + 1];
@@ -466,9 +533,14 @@ __global__ void __launch_bounds__(FLUX_THREADS, IMEX_FLUX_MINB)
     S.tile.info[ly][lx] = inf;
   }
   __syncthreads();
-  // interfaces: x faces (e < NXI) then y faces, one interface per thread
+  // interfaces: x faces (e < NXI), then y faces, one interface per thread;
+  // each direction's slopes are precomputed once per cell first
   const RingCell* rg = ring;
-  for (int e = threadIdx.x; e < NXI + NYI; e += blockDim.x) {
+  for (int pdir = 1; pdir <= 2; ++pdir) {
+  precompute_slopes<NS>(P, S.tile, S.slopes, pdir, j0, k0, mask);
+  __syncthreads();
+  for (int e = (pdir == 1 ? 0 : NXI) + threadIdx.x; e < (pdir == 1 ? NXI : NXI + NYI);
+       e += blockDim.x) {
     const int dir = (e < NXI) ? 1 : 2;
     int jj, kk, ja, ka, ia_x, ia_y;
     bool a_in, b_in, sa, sb_;
@@ -521,7 +593,7 @@ __global__ void __launch_bounds__(FLUX_THREADS, IMEX_FLUX_MINB)
     for (int pass = 0; pass < (dual ? 2 : 1); ++pass) {
       double Hp[NV];
       interface_flux<NS>(P, S.tile, dir, ia_x, ia_y, ja, ka, a_in, b_in, gcf, pass == 0, time, rg,
-                         Hp, amax, aN, aP);
+                         Hp, amax, aN, aP, &S.slopes);
       if (pass == 0) {
 #pragma unroll
         for (int i = 0; i < NV; ++i) H[i] = Hp[i];
@@ -537,6 +609,7 @@ __global__ void __launch_bounds__(FLUX_THREADS, IMEX_FLUX_MINB)
     a_slot = amax;
   }
   __syncthreads();
+  }
   // cells: divergence, explicit terms, CFL
   double dtl = P.max_dt;
   for (int e = threadIdx.x; e < TX * TY; e += blockDim.x) {
