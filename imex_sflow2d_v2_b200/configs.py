@@ -146,6 +146,26 @@ def topography_geom(B, dx, dy):
     return out
 
 
+def slope_correction_planes(geom):
+    """grav_coeff, d_grav_coeff_dx and the staggered grav_coeff from the
+    *_geom derivatives (src/geometry_2d.f90:827-847)."""
+    bx, by = geom["B_prime_x_geom"], geom["B_prime_y_geom"]
+    bxx, bxy = geom["B_second_xx_geom"], geom["B_second_xy_geom"]
+    gc = 1.0 / (1.0 + bx * bx + by * by)
+    dgc = -(2.0 * (gc * gc) * (bx * bxx + by * bxy))
+    nx, ny = gc.shape
+    sx = np.empty((nx + 1, ny))
+    sx[0] = gc[0]
+    sx[1:nx] = 0.5 * (gc[:-1] + gc[1:])
+    sx[nx] = gc[nx - 1]
+    sy = np.empty((nx, ny + 1))
+    sy[:, 0] = gc[:, 0]
+    sy[:, 1:ny] = 0.5 * (gc[:, :-1] + gc[:, 1:])
+    sy[:, ny] = gc[:, ny - 1]
+    return {"grav_coeff": np.asfortranarray(gc), "d_grav_coeff_dx": np.asfortranarray(dgc),
+            "grav_coeff_stag_x": np.asfortranarray(sx), "grav_coeff_stag_y": np.asfortranarray(sy)}
+
+
 def init_radial_source(p, x_source, y_source, r_source):
     """Inlet cells of a circular radial source: init_source
     (src/geometry_2d.f90:872-1102, radial branch).  Returns the planes

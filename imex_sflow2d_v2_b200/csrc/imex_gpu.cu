@@ -258,6 +258,23 @@ cudaError_t launch_erosion(ImexCtx* ctx) {
   }
 }
 
+// topography_reconstruction on the device after a bed change
+cudaError_t launch_topo(ImexCtx* ctx) {
+  const DevParams& P = ctx->P;
+  const long long n = (long long)P.nx * P.ny;
+  k_topo_geom<<<grid_1d(n, 256), 256, 0, ctx->stream>>>(ctx->dP, ctx->Bcent, ctx->Bx, ctx->By,
+                                                         ctx->Bxx, ctx->Bxy, ctx->Byy);
+  ctx->launches += 1;
+  if (P.slope_correction_flag) {
+    const long long m = n + (long long)(P.nx + 1) * P.ny + (long long)P.nx * (P.ny + 1);
+    k_topo_gc<<<grid_1d(m, 256), 256, 0, ctx->stream>>>(ctx->dP, ctx->Bx, ctx->By, ctx->Bxx,
+                                                         ctx->Bxy, ctx->gc, ctx->dgc, ctx->gcsx,
+                                                         ctx->gcsy);
+    ctx->launches += 1;
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_post_sweep(ImexCtx* ctx, int init) {
   const DevParams& P = ctx->P;
   const int grid = grid_1d((long long)P.nx * P.ny, 128);
@@ -320,6 +337,7 @@ cudaError_t enqueue_step(ImexCtx* ctx) {
     ProfScope ps(ctx, KID_EROSION);
     if ((e = launch_erosion(ctx)) != cudaSuccess) return e;
   }
+  if (ctx->P.topo_change_flag && (e = launch_topo(ctx)) != cudaSuccess) return e;
   if (ctx->post_on && (e = launch_post_sweep(ctx, 0)) != cudaSuccess) return e;
   k_step_end<<<1, 1, 0, ctx->stream>>>(ctx->clk);
   ctx->launches += 1;
@@ -346,6 +364,10 @@ int validate(const ImexParams* p, std::string& why) {
       if (x->flag < 0 || x->flag > 2) { why = "boundary flag out of range 0..2"; return IMEX_EINVAL; }
   }
   if (!(p->cell_size > 0.0)) { why = "cell_size must be positive"; return IMEX_EINVAL; }
+  if (p->topo_change_flag && (p->nx < 5 || p->ny < 5)) {
+    why = "topography update needs at least 5 cells per direction";
+    return IMEX_EUNSUPPORTED;
+  }
   return IMEX_OK;
 }
 
@@ -551,6 +573,16 @@ int imex_gpu_create(const ImexParams* p, const ImexStatic* s, int device, ImexCt
     CK(upload_plane(ctx, ctx->Bxx, s->B_second_xx_geom, 0.0));
     CK(upload_plane(ctx, ctx->Bxy, s->B_second_xy_geom, 0.0));
     CK(upload_plane(ctx, ctx->Byy, s->B_second_yy_geom, 0.0));
+  }
+  if (P.topo_change_flag && !P.curvature_term_flag) {
+    // the bed-change update writes the second derivatives (grav_coeff's
+    // derivative needs them); the step reads them only with curvature on
+    CK(dalloc(&ctx->Bxx, plane));
+    CK(dalloc(&ctx->Bxy, plane));
+    CK(dalloc(&ctx->Byy, plane));
+    CK(cudaMemset(ctx->Bxx, 0, plane * sizeof(double)));
+    CK(cudaMemset(ctx->Bxy, 0, plane * sizeof(double)));
+    CK(cudaMemset(ctx->Byy, 0, plane * sizeof(double)));
   }
   if (P.slope_correction_flag) {
     CK(dalloc(&ctx->gc, plane));
@@ -1030,6 +1062,15 @@ int imex_gpu_post_init(ImexCtx* ctx, int n_thickness_levels, const double* thick
   if (ctx->graph_exec) { cudaGraphExecDestroy(ctx->graph_exec); ctx->graph_exec = nullptr; }
   if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
   ctx->post_on = true;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return IMEX_OK;
+}
+
+int imex_gpu_topography_reconstruction(ImexCtx* ctx) {
+  if (!ctx) return IMEX_EINVAL;
+  if (!ctx->Bcent) return fail(ctx, IMEX_EINVAL, "topography update: no B_cent plane");
+  CK(cudaSetDevice(ctx->device));
+  CK(launch_topo(ctx));
   CK(cudaStreamSynchronize(ctx->stream));
   return IMEX_OK;
 }

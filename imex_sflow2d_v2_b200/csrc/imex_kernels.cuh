@@ -1934,6 +1934,101 @@ __global__ void k_qp_out(const DevParams* __restrict__ Pp, const double* __restr
   }
 }
 
+// ==================================================== topography update
+// topography_reconstruction after a bed change (src/geometry_2d.f90:683-860):
+// the 5-point first and second derivatives of B_cent and the 25-point mixed
+// one on the cells 3..n-2, copied to the 2-cell border; with slope
+// correction, grav_coeff, its x derivative and its staggered values.  A cell
+// in the border takes the stencil of its nearest interior cell, which is
+// what the reference's copies leave there.
+__global__ void __launch_bounds__(256)
+    k_topo_geom(const DevParams* __restrict__ Pp, const double* __restrict__ B,
+                double* __restrict__ Bx, double* __restrict__ By, double* __restrict__ Bxx,
+                double* __restrict__ Bxy, double* __restrict__ Byy) {
+  const DevParams& P = *Pp;
+  const int nx = P.nx, ny = P.ny;
+  const long long n = (long long)nx * ny;
+  const double c1[5] = {-2.0, -1.0, 0.0, 1.0, 2.0};
+  const double c2[5] = {2.0, -1.0, -2.0, -1.0, 2.0};
+  const double n1x = 10.0 * P.dx, n1y = 10.0 * P.dy;
+  const double n2x = 7.0 * (P.dx * P.dx), n2y = 7.0 * (P.dy * P.dy);
+  const double nxy = (10.0 * P.dx) * (10.0 * P.dy);
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < n;
+       g += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(g % nx), k = (int)(g / nx);
+    const int js = min(max(j, 2), nx - 3), ks = min(max(k, 2), ny - 3);
+    auto b = [&](int jj, int kk) { return B[(size_t)kk * P.pitch + jj]; };
+    double px = 0.0, sxx = 0.0, py = 0.0, syy = 0.0;
+#pragma unroll
+    for (int t = 0; t < 5; ++t) {
+      px = px + c1[t] * b(js + t - 2, ks);
+      sxx = sxx + c2[t] * b(js + t - 2, ks);
+    }
+#pragma unroll
+    for (int t = 0; t < 5; ++t) {
+      py = py + c1[t] * b(js, ks + t - 2);
+      syy = syy + c2[t] * b(js, ks + t - 2);
+    }
+    double ws = 0.0;
+    for (int u = 0; u < 5; ++u)
+#pragma unroll
+      for (int t = 0; t < 5; ++t) ws = ws + c1[t] * c1[u] * b(js + t - 2, ks + u - 2);
+    const size_t c = (size_t)k * P.pitch + j;
+    Bx[c] = px / n1x;
+    By[c] = py / n1y;
+    if (Bxx) {
+      Bxx[c] = sxx / n2x;
+      Byy[c] = syy / n2y;
+      Bxy[c] = ws / nxy;
+    }
+  }
+}
+
+__device__ __forceinline__ double topo_gc(double bx, double by) {
+  return 1.0 / (1.0 + bx * bx + by * by);
+}
+
+__global__ void __launch_bounds__(256)
+    k_topo_gc(const DevParams* __restrict__ Pp, const double* __restrict__ Bx,
+              const double* __restrict__ By, const double* __restrict__ Bxx,
+              const double* __restrict__ Bxy, double* __restrict__ gc, double* __restrict__ dgc,
+              double* __restrict__ gcsx, double* __restrict__ gcsy) {
+  const DevParams& P = *Pp;
+  const int nx = P.nx, ny = P.ny;
+  const long long ncell = (long long)nx * ny, nsx = (long long)(nx + 1) * ny,
+                  nsy = (long long)nx * (ny + 1);
+  auto gcat = [&](int j, int k) {
+    const size_t c = (size_t)k * P.pitch + j;
+    return topo_gc(Bx[c], By[c]);
+  };
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < ncell + nsx + nsy;
+       g += (long long)gridDim.x * blockDim.x) {
+    if (g < ncell) {
+      const int j = (int)(g % nx), k = (int)(g / nx);
+      const size_t c = (size_t)k * P.pitch + j;
+      const double bx = Bx[c], by = By[c], gcv = topo_gc(bx, by);
+      gc[c] = gcv;
+      dgc[c] = -(2.0 * (gcv * gcv) * (bx * Bxx[c] + by * Bxy[c]));
+    } else if (g < ncell + nsx) {
+      const long long h = g - ncell;           // grav_coeff_stag_x(nx+1, ny)
+      const int j = (int)(h % (nx + 1)), k = (int)(h / (nx + 1));
+      double v;
+      if (j == 0) v = gcat(0, k);
+      else if (j == nx) v = gcat(nx - 1, k);
+      else v = 0.5 * (gcat(j - 1, k) + gcat(j, k));
+      gcsx[(size_t)k * (nx + 1) + j] = v;
+    } else {
+      const long long h = g - ncell - nsx;     // grav_coeff_stag_y(nx, ny+1)
+      const int j = (int)(h % nx), k = (int)(h / nx);
+      double v;
+      if (k == 0) v = gcat(j, 0);
+      else if (k == ny) v = gcat(j, ny - 1);
+      else v = 0.5 * (gcat(j, k - 1) + gcat(j, k));
+      gcsy[(size_t)k * nx + j] = v;
+    }
+  }
+}
+
 // ============================================================= post step
 // The driver's output sweep over the solve cells after each step
 // (src/IMEX_SfloW2D.f90:391-442) and its first form after the initial

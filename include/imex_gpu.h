@@ -203,6 +203,13 @@ int imex_gpu_timestep(ImexCtx* ctx, double* dt);
 int imex_gpu_timestep_noalloc(ImexCtx* ctx, double* dt);
 int imex_gpu_rk_step(ImexCtx* ctx, double t, double dt);
 int imex_gpu_erosion_deposition(ImexCtx* ctx, double dt);
+/* topography_reconstruction (src/geometry_2d.f90:535-860) on the device from
+ * the context's B_cent: the *_geom slopes and curvatures the step reads and,
+ * with slope correction, grav_coeff, d_grav_coeff_dx and the staggered
+ * grav_coeff.  imex_gpu_advance runs it after every step when
+ * topo_change_flag is set (as the driver does, src/IMEX_SfloW2D.f90:387);
+ * with topo_change_flag the grid needs at least 5 cells per direction. */
+int imex_gpu_topography_reconstruction(ImexCtx* ctx);
 
 /* Masks back to the host: solve_mask (nx,ny), solve_mask_x (nx+1,ny),
  * solve_mask_y (nx,ny+1); 0/1 bytes.  Any pointer may be NULL. */

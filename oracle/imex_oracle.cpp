@@ -331,6 +331,7 @@ struct OracleCtx {
   std::vector<double> hmax, pdynmax, mvmax;
   std::vector<uint8_t> vuln;  // (n_thk*n_pdyn, cell)
   void post_cell(int j, int k, bool init);
+  void topography_reconstruction();
 };
 
 // ------------------------------------------------------------------ mixt_var
@@ -2052,6 +2053,76 @@ void OracleCtx::post_step_sweep() {
   }
 }
 
+// src/geometry_2d.f90:683-860: the *_geom derivatives of B_cent (5-point
+// stencils on cells 3..n-2 in the reference's summation order, then the
+// border copies, columns before rows) and, with slope correction, grav_coeff,
+// d_grav_coeff_dx and the staggered grav_coeff.
+void OracleCtx::topography_reconstruction() {
+  const double cf1[5] = {-2.0, -1.0, 0.0, 1.0, 2.0};
+  const double cf2[5] = {2.0, -1.0, -2.0, -1.0, 2.0};
+  const double norm1_x = 10.0 * dx, norm1_y = 10.0 * dy;
+  const double norm2_x = 7.0 * (dx * dx), norm2_y = 7.0 * (dy * dy);
+  const double norm_xy = (10.0 * dx) * (10.0 * dy);
+  const size_t N = (size_t)nx * ny;
+  if (Bxx.empty()) Bxx.assign(N, 0.0);
+  if (Bxy.empty()) Bxy.assign(N, 0.0);
+  if (Byy.empty()) Byy.assign(N, 0.0);
+  auto B = [&](int j, int k) { return B_cent[c2(j, k)]; };
+  for (int k = 3; k <= ny - 2; ++k)
+    for (int j = 3; j <= nx - 2; ++j) {
+      double px = 0.0, sxx = 0.0, py = 0.0, syy = 0.0;
+      for (int kj = 1; kj <= 5; ++kj) {
+        px = px + cf1[kj - 1] * B(j + kj - 3, k);
+        sxx = sxx + cf2[kj - 1] * B(j + kj - 3, k);
+      }
+      for (int kk = 1; kk <= 5; ++kk) {
+        py = py + cf1[kk - 1] * B(j, k + kk - 3);
+        syy = syy + cf2[kk - 1] * B(j, k + kk - 3);
+      }
+      const size_t c = c2(j, k);
+      Bx[c] = px / norm1_x;
+      By[c] = py / norm1_y;
+      Bxx[c] = sxx / norm2_x;
+      Byy[c] = syy / norm2_y;
+      double ws = 0.0;
+      for (int kk = 1; kk <= 5; ++kk)
+        for (int kj = 1; kj <= 5; ++kj) ws = ws + cf1[kj - 1] * cf1[kk - 1] * B(j + kj - 3, k + kk - 3);
+      Bxy[c] = ws / norm_xy;
+    }
+  std::vector<double>* planes[5] = {&Bx, &By, &Bxx, &Byy, &Bxy};
+  for (auto* pl : planes) {
+    std::vector<double>& a = *pl;
+    for (int k = 1; k <= ny; ++k) {
+      a[c2(1, k)] = a[c2(3, k)];
+      a[c2(2, k)] = a[c2(3, k)];
+      a[c2(nx - 1, k)] = a[c2(nx - 2, k)];
+      a[c2(nx, k)] = a[c2(nx - 2, k)];
+    }
+    for (int j = 1; j <= nx; ++j) {
+      a[c2(j, 1)] = a[c2(j, 3)];
+      a[c2(j, 2)] = a[c2(j, 3)];
+      a[c2(j, ny - 1)] = a[c2(j, ny - 2)];
+      a[c2(j, ny)] = a[c2(j, ny - 2)];
+    }
+  }
+  if (p.slope_correction_flag) {
+    for (size_t c = 0; c < N; ++c) {
+      gc[c] = 1.0 / (1.0 + Bx[c] * Bx[c] + By[c] * By[c]);
+      dgc_dx[c] = -(2.0 * (gc[c] * gc[c]) * (Bx[c] * Bxx[c] + By[c] * Bxy[c]));
+    }
+    for (int k = 1; k <= ny; ++k) {
+      gc_sx[sx2(1, k)] = gc[c2(1, k)];
+      for (int j = 2; j <= nx; ++j) gc_sx[sx2(j, k)] = 0.5 * (gc[c2(j - 1, k)] + gc[c2(j, k)]);
+      gc_sx[sx2(nx + 1, k)] = gc[c2(nx, k)];
+    }
+    for (int j = 1; j <= nx; ++j) {
+      gc_sy[sy2(j, 1)] = gc[c2(j, 1)];
+      for (int k = 2; k <= ny; ++k) gc_sy[sy2(j, k)] = 0.5 * (gc[c2(j, k - 1)] + gc[c2(j, k)]);
+      gc_sy[sy2(j, ny + 1)] = gc[c2(j, ny)];
+    }
+  }
+}
+
 // One cell of the driver's output sweep: qp, running maxima and the
 // vulnerability table (src/IMEX_SfloW2D.f90:398-440; init: :261-307).
 void OracleCtx::post_cell(int j, int k, bool init) {
@@ -2362,6 +2433,7 @@ uint32_t oracle_advance(OracleCtx* o, int n_steps, double* t) {
     for (int b = 0; b < 16; ++b) o->hist[b] = 0;
     err |= o->imex_RK_solver(dt);
     err |= o->update_erosion_deposition_cell(dt);
+    if (o->p.topo_change_flag) o->topography_reconstruction();
     o->t = o->t + dt;
     o->post_step_sweep();
     o->steps += 1;
@@ -2488,4 +2560,20 @@ extern "C" void oracle_get_post(OracleCtx* o, double* hmax, double* pdynmax, dou
   }
   if (vuln)
     for (size_t i = 0; i < o->vuln.size(); ++i) vuln[i] = (int8_t)o->vuln[i];
+}
+
+extern "C" void oracle_topography_reconstruction(OracleCtx* o) { o->topography_reconstruction(); }
+
+extern "C" void oracle_get_topo(OracleCtx* o, double* bx, double* by, double* bxx, double* bxy,
+                                double* byy, double* gc, double* dgc) {
+  const size_t N = (size_t)o->nx * o->ny;
+  for (size_t c = 0; c < N; ++c) {
+    if (bx) bx[c] = o->Bx[c];
+    if (by) by[c] = o->By[c];
+    if (bxx && !o->Bxx.empty()) bxx[c] = o->Bxx[c];
+    if (bxy && !o->Bxy.empty()) bxy[c] = o->Bxy[c];
+    if (byy && !o->Byy.empty()) byy[c] = o->Byy[c];
+    if (gc) gc[c] = o->gc[c];
+    if (dgc) dgc[c] = o->dgc_dx[c];
+  }
 }

@@ -68,6 +68,8 @@ def lib():
         L.oracle_post_init.argtypes = [vp, C.c_int, dp, C.c_int, dp]
         L.oracle_post_diag.argtypes = [vp, dp]
         L.oracle_get_post.argtypes = [vp, dp, dp, dp, C.POINTER(C.c_int8)]
+        L.oracle_topography_reconstruction.argtypes = [vp]
+        L.oracle_get_topo.argtypes = [vp] + [dp] * 7
         L.oracle_limit.restype = C.c_double
         L.oracle_limit.argtypes = [C.c_double] * 6 + [C.c_int, C.c_double]
         _LIB = L
@@ -186,6 +188,16 @@ class Oracle:
                               v.ctypes.data_as(C.POINTER(C.c_int8)))
         f = [x.reshape((self.nx, self.ny), order="F") for x in a]
         return f[0], f[1], f[2], v[:self._nt * n].reshape((self._nt, self.nx, self.ny), order="F")
+
+    def topography_reconstruction(self):
+        lib().oracle_topography_reconstruction(self._h)
+
+    def get_topo(self):
+        """B_prime_x/y_geom, B_second_xx/xy/yy_geom, grav_coeff, d_grav_coeff_dx."""
+        n = self.nx * self.ny
+        a = [np.zeros(n) for _ in range(7)]
+        lib().oracle_get_topo(self._h, *[_p(x) for x in a])
+        return [x.reshape((self.nx, self.ny), order="F") for x in a]
 
     # point functions
     def qc_to_qp(self, qc):

@@ -203,3 +203,18 @@ def edge_variants():
     # smallest grid the path accepts
     out["tiny_3x5"] = configs.dambreak(nx=3, ny=5, dx=0.25, rheology=1, x_split=0.4)
     return out
+
+
+def fractal_topo(n=48):
+    """The fractal workload with a moving bed: erosion and deposition change
+    B_cent (topo_change_flag), the slopes and, with slope correction and
+    curvature on, grav_coeff and the curvatures are rebuilt after every step."""
+    p, st, q = configs.fractal_inlet(n=n, initial_layer=1.0, erosion_coeff=5.0e-3)
+    p.topo_change_flag = 1
+    p.slope_correction_flag = 1
+    p.curvature_term_flag = 1
+    st = dict(st)
+    geo = configs.topography_geom(np.asarray(st["B_cent"]), p.cell_size, p.cell_size)
+    st.update(geo)
+    st.update(configs.slope_correction_planes(geo))
+    return p, st, q

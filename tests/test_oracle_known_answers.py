@@ -152,3 +152,27 @@ def test_ipow_accuracy_and_special_values():
             assert abs(ipow(x, y) - exact) <= 4 * math.ulp(exact), (x, y)
     assert ipow(1.0, 1.5) == 1.0 and ipow(0.0, 0.5) == 0.0 and ipow(2.0, 0.0) == 1.0
     assert math.isnan(ipow(-1.0, 0.5)) and ipow(-1.0, 0.0) == 1.0
+
+
+def test_topography_reconstruction_matches_numpy_stencils():
+    """The oracle's topography_reconstruction (reference summation order)
+    against the independent numpy stencils of configs.topography_geom and
+    configs.slope_correction_planes, on a rough seeded bed."""
+    p, st, q = configs.dambreak(nx=23, ny=17, dx=0.7, rheology=1)
+    rng = np.random.default_rng(9)
+    B = np.asfortranarray(rng.standard_normal((23, 17)) * 3.0 + np.arange(23)[:, None] * 0.4)
+    st = dict(st)
+    st["B_cent"] = B
+    p.slope_correction_flag = 1
+    geo = configs.topography_geom(B, 0.7, 0.7)
+    st.update(configs.slope_correction_planes(geo))
+    o = Oracle(p, st, threads=1)
+    o.topography_reconstruction()
+    bx, by, bxx, bxy, byy, gc, dgc = o.get_topo()
+    ref = [geo["B_prime_x_geom"], geo["B_prime_y_geom"], geo["B_second_xx_geom"],
+           geo["B_second_xy_geom"], geo["B_second_yy_geom"]]
+    for a, b in zip((bx, by, bxx, bxy, byy), ref):
+        np.testing.assert_allclose(a, b, rtol=1e-12, atol=1e-12)
+    sc = configs.slope_correction_planes(geo)
+    np.testing.assert_allclose(gc, sc["grav_coeff"], rtol=1e-12)
+    np.testing.assert_allclose(dgc, sc["d_grav_coeff_dx"], rtol=1e-10, atol=1e-14)
