@@ -20,6 +20,8 @@
 
 #include <cstdint>
 
+#include "ipow_tables.h"
+
 #ifndef IMEX_HD
 #define IMEX_HD __device__ __forceinline__
 #endif
@@ -94,17 +96,19 @@ IMEX_HD double fmax_f(double a, double b) {
 // x**y for the non-integer exponents of the mass-exchange closures
 // (settling drag, hindered settling, entrainment, inlet ramps).  Both the CPU
 // oracle and the CUDA path evaluate it with this same sequence of IEEE
-// operations, so the two agree bit for bit; the sequence is
-//   log x = e*ln2 + 2*atanh(s), s = (m-1)/(m+1), m in [sqrt(1/2), sqrt(2)),
-//           atanh by its odd Taylor series to s^23 (Horner with fused
-//           multiply-adds),
+// operations and the same tables (ipow_tables.h), so the two agree bit for
+// bit; the sequence is
+//   log x = e*ln2 - log(invc_i) + log1p(r): m in [1,2), i its top 7 fraction
+//           bits, r = m*invc_i - 1 by one fused multiply-add (|r| < 2^-8),
+//           log1p(r) by its Taylor series to r^7, -log(invc_i) tabulated as a
+//           sum of two doubles,
 //   z = y*log x carried as an unevaluated sum of two doubles (exact product
 //       error by one fused multiply-add, Knuth's two-sum),
-//   exp z = 2^k * exp(r), r = z - k*ln2 (ln2 split in two), exp(r) by its
-//           Taylor series to r^14 (Horner with fused multiply-adds).
+//   exp z = 2^(k/64) * exp(r), r = z - k*ln2/64 (ln2/64 split in two),
+//           exp(r) - 1 by its Taylor series to r^6, 2^(j/64) tabulated.
 // Every fused multiply-add is the IEEE single-rounding operation on both
-// sides (CUDA fma, C++ std::fma), so the bits stay identical.
-// Accuracy against the exact power: within 4 ulp (measured); the reference's
+// sides (CUDA fma, C++ std::fma).
+// Accuracy against the exact power: within 0.52 ulp (tested); the reference's
 // libm pow is within 1 ulp, so results differ from it at that level only.
 IMEX_HD void two_sum(double a, double b, double& s, double& e) {
   s = a + b;
@@ -123,27 +127,26 @@ IMEX_NOINL double ipow(double x, double y) {
   if (y == 0.0) return 1.0;
   if (x == 1.0) return 1.0;
   const double LN2_HI = 0x1.62e42fee00000p-1, LN2_LO = 0x1.a39ef35793c76p-33;
-  const double INV_LN2 = 0x1.71547652b82fep+0, SQRTH = 0x1.6a09e667f3bcdp-1;
+  const double LN2_64_HI = 0x1.62e42fee00000p-7, LN2_64_LO = 0x1.a39ef35793c76p-39;
+  const double INV_LN2_64 = 0x1.71547652b82fep+6;
+  // log x = e*ln2 - log(invc_i) + log1p(r), m*invc_i = 1 + r, |r| < 2^-8
   int e;
-  double m = frexp(x, &e);
-  if (m < SQRTH) {
-    m = m * 2.0;
-    e = e - 1;
-  }
-  double f = m - 1.0;
-  double s = f / (2.0 + f);
-  double s2 = s * s;
-  const double inv_odd[11] = {0x1.5555555555555p-2, 0x1.999999999999ap-3, 0x1.2492492492492p-3,
-                                     0x1.c71c71c71c71cp-4, 0x1.745d1745d1746p-4, 0x1.3b13b13b13b14p-4,
-                                     0x1.1111111111111p-4, 0x1.e1e1e1e1e1e1ep-5, 0x1.af286bca1af28p-5,
-                                     0x1.8618618618618p-5, 0x1.642c8590b2164p-5};
-  double P = inv_odd[10];
-  for (int k = 9; k >= 0; --k) P = fma(s2, P, inv_odd[k]);
-  double ts = 2.0 * s;
-  double logm = fma(ts, s2 * P, ts);
-  double hi, lo;
-  two_sum((double)e * LN2_HI, logm, hi, lo);
-  lo = lo + (double)e * LN2_LO;
+  double m = frexp(x, &e);          // m in [1/2, 1)
+  m = m * 2.0;
+  e = e - 1;
+  const int i = (int)((m - 1.0) * 128.0);
+  const double r = fma(m, IPOW_INVC[i], -1.0);
+  double P = fma(r, 0x1.2492492492492p-3, -0x1.5555555555555p-3);   // 1/7, -1/6
+  P = fma(r, P, 0x1.999999999999ap-3);                               // 1/5
+  P = fma(r, P, -0x1.0000000000000p-2);                              // -1/4
+  P = fma(r, P, 0x1.5555555555555p-2);                               // 1/3
+  P = fma(r, P, -0x1.0000000000000p-1);                              // -1/2
+  const double l1p = fma(r * r, P, r);
+  double a, b, hi, c;
+  two_sum((double)e * LN2_HI, IPOW_LOGC_HI[i], a, b);
+  two_sum(a, l1p, hi, c);
+  double lo = ((b + c) + IPOW_LOGC_LO[i]) + (double)e * LN2_LO;
+  // z = y*log x in double-double
   double p, pe;
   two_prod(y, hi, p, pe);
   pe = fma(y, lo, pe);
@@ -151,18 +154,21 @@ IMEX_NOINL double ipow(double x, double y) {
   two_sum(p, pe, zh, zl);
   if (zh > 709.78) return __longlong_as_double(0x7ff0000000000000LL);
   if (zh < -745.1) return 0.0;
-  double kf = rint(zh * INV_LN2);
+  // exp z = 2^(k/64) exp(rr), |rr| < ln2/128
+  const double kf = rint(zh * INV_LN2_64);
+  const long long k = (long long)kf;
+  const int j = (int)(k & 63);
+  const int me = (int)((k - j) / 64);
   double rh, rl;
-  two_sum(zh, -(kf * LN2_HI), rh, rl);
-  double r = rh + (rl + fma(-kf, LN2_LO, zl));
-  const double fact[15] = {0x1.0000000000000p+0, 0x1.0000000000000p+0, 0x1.0000000000000p-1,
-                                  0x1.5555555555555p-3, 0x1.5555555555555p-5, 0x1.1111111111111p-7,
-                                  0x1.6c16c16c16c17p-10, 0x1.a01a01a01a01ap-13, 0x1.a01a01a01a01ap-16,
-                                  0x1.71de3a556c734p-19, 0x1.27e4fb7789f5cp-22, 0x1.ae64567f544e4p-26,
-                                  0x1.1eed8eff8d898p-29, 0x1.6124613a86d09p-33, 0x1.93974a8c07c9dp-37};
-  double E = fact[14];
-  for (int k = 13; k >= 0; --k) E = fma(r, E, fact[k]);
-  return ldexp(E, (int)kf);
+  two_sum(zh, -(kf * LN2_64_HI), rh, rl);
+  const double rr = rh + (rl + fma(-kf, LN2_64_LO, zl));
+  double E = fma(rr, 0x1.6c16c16c16c17p-10, 0x1.1111111111111p-7);  // 1/720, 1/120
+  E = fma(rr, E, 0x1.5555555555555p-5);                              // 1/24
+  E = fma(rr, E, 0x1.5555555555555p-3);                              // 1/6
+  E = fma(rr, E, 0x1.0000000000000p-1);                              // 1/2
+  const double em1 = fma(rr * rr, E, rr);
+  const double th = IPOW_EXP2_HI[j];
+  return ldexp(th + fma(th, em1, IPOW_EXP2_LO[j]), me);
 }
 
 // ------------------------------------------------------------- complex
