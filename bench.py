@@ -346,13 +346,11 @@ def main():
     kt = g.kernel_times()
     g.profile(False)
     s1 = g.stats()
+    from imex_sflow2d_v2_b200.replicas import job_rate
+    value, sec = job_rate(ms * 1e-3, cells * args.steps, dist, "cuda")
+    ms = sec * 1e3
     if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        if dist:
-            dist.barrier()
-    value = world * cells * args.steps / (ms * 1e-3)
+        dist.barrier()
     launches = int(s1.kernel_launches - s0.kernel_launches)
     newton_per_cell = s1.newton_iters / max(1, s1.newton_cells)
 
@@ -415,11 +413,8 @@ def main():
             g.get_state(out=hq)
         g.sync()
         el = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([el], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
-        e2e = {"value": world * cells * args.e2e_steps / el, "unit": UNIT,
+        e2e_rate, el = job_rate(el, cells * args.e2e_steps, dist, "cuda")
+        e2e = {"value": e2e_rate, "unit": UNIT,
                "h2d_bytes_per_step": nv * cells * 8, "d2h_bytes_per_step": nv * cells * 8,
                "steps": args.e2e_steps}
 
