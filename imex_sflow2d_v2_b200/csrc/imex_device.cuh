@@ -72,6 +72,9 @@ struct DevParams {
   double erodible_fract[MAXS], rho_c_sub, coeff_porosity;
   int n_ring;             // inlet ring cells (source_cell == 2)
 };
+// Kernels take DevParams by value (a __grid_constant__ parameter): its
+// fields are read from the constant bank, not from global memory.
+static_assert(sizeof(DevParams) <= 2048, "DevParams must fit the kernel parameter space");
 
 // cellinfo bits
 constexpr uint8_t CI_SRC_MASK = 3;   // source_cell value 0/1/2

@@ -163,7 +163,7 @@ cudaError_t launch_flux_ns(ImexCtx* ctx) {
     attr_set = true;
   }
   k_flux<NS><<<tile_grid(P), FLUX_THREADS, smem, ctx->stream>>>(
-      ctx->dP, ctx->q, ctx->mask, ctx->cellinfo, ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy, ctx->Byy,
+      ctx->P, ctx->q, ctx->mask, ctx->cellinfo, ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy, ctx->Byy,
       ctx->gc, ctx->dgc, ctx->gcsx, ctx->gcsy, ctx->ring, ctx->clk, ctx->X);
   ctx->launches += 1;
   return cudaGetLastError();
@@ -191,38 +191,38 @@ cudaError_t launch_stage2_ns(ImexCtx* ctx) {
   {
     ProfScope ps(ctx, KID_S2_FIRST);
     k_stage2_first<NS><<<grid, STAGE2_THREADS, 0, ctx->stream>>>(
-        ctx->dP, ctx->q, ctx->X, ctx->mask, ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy, ctx->Byy,
+        ctx->P, ctx->q, ctx->X, ctx->mask, ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy, ctx->Byy,
         ctx->gc, ctx->nw, ctx->clk);
     if (ctx->nw.warm) {
       cudaError_t e = launch_warm_predict(ctx);
       if (e != cudaSuccess) return e;
-      k_stage2_wstart<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->Bx,
+      k_stage2_wstart<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->Bx,
                                                                      ctx->By, ctx->nw, ctx->clk);
       ctx->launches += 1;
     }
   }
   {
     ProfScope ps(ctx, KID_S2_ITER);
-    k_stage2_iter<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->Bx,
+    k_stage2_iter<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->Bx,
                                                                  ctx->By, ctx->nw, ctx->clk, 2);
-    k_stage2_iter<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->Bx,
+    k_stage2_iter<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->Bx,
                                                                  ctx->By, ctx->nw, ctx->clk, 3);
-    k_stage2_tail<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->Bx,
+    k_stage2_tail<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->Bx,
                                                                  ctx->By, ctx->nw, ctx->clk);
     if (ctx->nw.warm) {
-      k_stage2_fallback<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->Bx,
+      k_stage2_fallback<NS><<<lgrid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->Bx,
                                                                        ctx->By, ctx->nw, ctx->clk);
       ctx->launches += 1;
     }
   }
   if (ctx->nw.harvest) {
-    k_harvest<NS><<<grid_1d(ncell, 128), 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->Bx, ctx->By,
+    k_harvest<NS><<<grid_1d(ncell, 128), 128, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->Bx, ctx->By,
                                                                 ctx->nw, ctx->clk);
     ctx->launches += 1;
   }
   {
     ProfScope ps(ctx, KID_S2_POST);
-    k_stage2_post<NS><<<grid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->mask,
+    k_stage2_post<NS><<<grid, STAGE2_THREADS, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->mask,
                                                                 ctx->cellinfo, ctx->nw, ctx->clk);
   }
   ctx->launches += 6;
@@ -242,7 +242,7 @@ template <int NS>
 cudaError_t launch_erosion_ns(ImexCtx* ctx) {
   const DevParams& P = ctx->P;
   int grid = grid_1d((long long)P.nx * P.ny, 128);
-  k_erosion<NS><<<grid, 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->mask, ctx->Bx, ctx->By,
+  k_erosion<NS><<<grid, 128, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->mask, ctx->Bx, ctx->By,
                                                ctx->erodible, ctx->deposit, ctx->erosion,
                                                ctx->Bcent, ctx->clk);
   ctx->launches += 1;
@@ -262,12 +262,12 @@ cudaError_t launch_erosion(ImexCtx* ctx) {
 cudaError_t launch_topo(ImexCtx* ctx) {
   const DevParams& P = ctx->P;
   const long long n = (long long)P.nx * P.ny;
-  k_topo_geom<<<grid_1d(n, 256), 256, 0, ctx->stream>>>(ctx->dP, ctx->Bcent, ctx->Bx, ctx->By,
+  k_topo_geom<<<grid_1d(n, 256), 256, 0, ctx->stream>>>(ctx->P, ctx->Bcent, ctx->Bx, ctx->By,
                                                          ctx->Bxx, ctx->Bxy, ctx->Byy);
   ctx->launches += 1;
   if (P.slope_correction_flag) {
     const long long m = n + (long long)(P.nx + 1) * P.ny + (long long)P.nx * (P.ny + 1);
-    k_topo_gc<<<grid_1d(m, 256), 256, 0, ctx->stream>>>(ctx->dP, ctx->Bx, ctx->By, ctx->Bxx,
+    k_topo_gc<<<grid_1d(m, 256), 256, 0, ctx->stream>>>(ctx->P, ctx->Bx, ctx->By, ctx->Bxx,
                                                          ctx->Bxy, ctx->gc, ctx->dgc, ctx->gcsx,
                                                          ctx->gcsy);
     ctx->launches += 1;
@@ -279,10 +279,10 @@ cudaError_t launch_post_sweep(ImexCtx* ctx, int init) {
   const DevParams& P = ctx->P;
   const int grid = grid_1d((long long)P.nx * P.ny, 128);
   switch (ctx->ns) {
-    case 1: k_post_sweep<1><<<grid, 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->mask, ctx->post, ctx->post_levels, init); break;
-    case 2: k_post_sweep<2><<<grid, 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->mask, ctx->post, ctx->post_levels, init); break;
-    case 3: k_post_sweep<3><<<grid, 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->mask, ctx->post, ctx->post_levels, init); break;
-    default: k_post_sweep<4><<<grid, 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->mask, ctx->post, ctx->post_levels, init); break;
+    case 1: k_post_sweep<1><<<grid, 128, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->mask, ctx->post, ctx->post_levels, init); break;
+    case 2: k_post_sweep<2><<<grid, 128, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->mask, ctx->post, ctx->post_levels, init); break;
+    case 3: k_post_sweep<3><<<grid, 128, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->mask, ctx->post, ctx->post_levels, init); break;
+    default: k_post_sweep<4><<<grid, 128, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->mask, ctx->post, ctx->post_levels, init); break;
   }
   ctx->launches += 1;
   return cudaGetLastError();
@@ -293,10 +293,10 @@ constexpr int DIAG_BLOCKS = 148 * 4;
 cudaError_t launch_post_diag(ImexCtx* ctx) {
   double* part = ctx->post_diag + 4;
   switch (ctx->ns) {
-    case 1: k_post_diag<1><<<DIAG_BLOCKS, DIAG_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->post.qp_h, part); break;
-    case 2: k_post_diag<2><<<DIAG_BLOCKS, DIAG_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->post.qp_h, part); break;
-    case 3: k_post_diag<3><<<DIAG_BLOCKS, DIAG_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->post.qp_h, part); break;
-    default: k_post_diag<4><<<DIAG_BLOCKS, DIAG_THREADS, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->post.qp_h, part); break;
+    case 1: k_post_diag<1><<<DIAG_BLOCKS, DIAG_THREADS, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->post.qp_h, part); break;
+    case 2: k_post_diag<2><<<DIAG_BLOCKS, DIAG_THREADS, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->post.qp_h, part); break;
+    case 3: k_post_diag<3><<<DIAG_BLOCKS, DIAG_THREADS, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->post.qp_h, part); break;
+    default: k_post_diag<4><<<DIAG_BLOCKS, DIAG_THREADS, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->post.qp_h, part); break;
   }
   k_post_diag_fold<<<1, 32, 0, ctx->stream>>>(part, DIAG_BLOCKS, ctx->post_diag);
   ctx->launches += 2;
@@ -305,7 +305,7 @@ cudaError_t launch_post_diag(ImexCtx* ctx) {
 
 cudaError_t launch_mask(ImexCtx* ctx, int solve_all = 0) {
   const DevParams& P = ctx->P;
-  k_mask<<<tile_grid(P), 256, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->release, ctx->cellinfo,
+  k_mask<<<tile_grid(P), 256, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->release, ctx->cellinfo,
                                                 ctx->clk, ctx->mask, ctx->clk, solve_all);
   ctx->launches += 1;
   return cudaGetLastError();
@@ -698,10 +698,10 @@ int imex_gpu_get_state(ImexCtx* ctx, double* q, double* qp) {
   }
   if (qp) {
     switch (ctx->ns) {
-      case 1: k_qp_out<1><<<grid_1d((long long)N, 128), 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->scratch, ctx->cellinfo); break;
-      case 2: k_qp_out<2><<<grid_1d((long long)N, 128), 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->scratch, ctx->cellinfo); break;
-      case 3: k_qp_out<3><<<grid_1d((long long)N, 128), 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->scratch, ctx->cellinfo); break;
-      default: k_qp_out<4><<<grid_1d((long long)N, 128), 128, 0, ctx->stream>>>(ctx->dP, ctx->q, ctx->scratch, ctx->cellinfo); break;
+      case 1: k_qp_out<1><<<grid_1d((long long)N, 128), 128, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->scratch, ctx->cellinfo); break;
+      case 2: k_qp_out<2><<<grid_1d((long long)N, 128), 128, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->scratch, ctx->cellinfo); break;
+      case 3: k_qp_out<3><<<grid_1d((long long)N, 128), 128, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->scratch, ctx->cellinfo); break;
+      default: k_qp_out<4><<<grid_1d((long long)N, 128), 128, 0, ctx->stream>>>(ctx->P, ctx->q, ctx->scratch, ctx->cellinfo); break;
     }
     ctx->launches += 1;
     CK(cudaGetLastError());
@@ -819,7 +819,7 @@ int imex_gpu_get_masks(ImexCtx* ctx, int8_t* solve_mask, int8_t* mask_x, int8_t*
   if (mask_x || mask_y) {
     size_t nX = (size_t)(nx + 1) * ny, nY = (size_t)nx * (ny + 1);
     int8_t* d = reinterpret_cast<int8_t*>(ctx->scratch);
-    k_masks_xy<<<grid_1d((long long)(nX + nY), 256), 256, 0, ctx->stream>>>(ctx->dP, ctx->mask, d, d + nX);
+    k_masks_xy<<<grid_1d((long long)(nX + nY), 256), 256, 0, ctx->stream>>>(ctx->P, ctx->mask, d, d + nX);
     ctx->launches += 1;
     CK(cudaGetLastError());
     if (mask_x) CK(cudaMemcpyAsync(mask_x, d, nX, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1390,7 +1390,7 @@ cudaError_t launch_warm_predict_ns(ImexCtx* ctx) {
     nrm.y_std[i] = n[2 * WARM_IN + WARM_OUT + i];
   }
   k_warm_predict<NS><<<148 * 2, 32 * mlp::WARPS, mlp::SMEM_NET, ctx->stream>>>(
-      ctx->dP, ctx->nw, ctx->clk, ctx->warm_mlp->bw, ctx->warm_mlp->prm, nrm);
+      ctx->P, ctx->nw, ctx->clk, ctx->warm_mlp->bw, ctx->warm_mlp->prm, nrm);
   ctx->launches += 1;
   return cudaGetLastError();
 }
@@ -1748,12 +1748,12 @@ double* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
 // view everywhere gives the same speeds.  The fluxes are discarded.
 template <int NS>
 __global__ void __launch_bounds__(FLUX_THREADS)
-    k_cfl_tiles(const DevParams* __restrict__ Pp, const double* __restrict__ q,
+    k_cfl_tiles(const __grid_constant__ DevParams Pp, const double* __restrict__ q,
                 const uint8_t* __restrict__ mask, const uint8_t* __restrict__ cellinfo,
                 const double* __restrict__ gcsx, const double* __restrict__ gcsy,
                 const RingCell* __restrict__ ring, const DevClock* clk, double* tile_min) {
   constexpr int NV = 4 + NS, NP = 6 + NS;
-  const DevParams& P = *Pp;
+  const DevParams& P = Pp;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   FluxShared<NS>& S = *reinterpret_cast<FluxShared<NS>*>(smem_raw);
   const int j0 = blockIdx.x * TX, k0 = blockIdx.y * TY;
@@ -1852,10 +1852,10 @@ __global__ void __launch_bounds__(FLUX_THREADS)
 
 // One block folds the tile minima into slot n_tiles of the same array with
 // the rule of the atomic minimum in k_flux (only 0 <= m < max_dt lowers dt).
-__global__ void __launch_bounds__(1024) k_cfl_fold(const DevParams* __restrict__ Pp,
+__global__ void __launch_bounds__(1024) k_cfl_fold(const __grid_constant__ DevParams Pp,
                                                    double* tile_min, long long n_tiles) {
   __shared__ double red[32];
-  const double max_dt = Pp->max_dt;
+  const double max_dt = Pp.max_dt;
   double m = max_dt;
   for (long long i = threadIdx.x; i < n_tiles; i += blockDim.x) {
     double v = tile_min[i];
@@ -1879,7 +1879,7 @@ cudaError_t launch_cfl_tiles(ImexCtx* ctx, double* scratch) {
                                        (int)smem);
   if (e != cudaSuccess) return e;
   k_cfl_tiles<NS><<<tile_grid(P), FLUX_THREADS, smem, ctx->stream>>>(
-      ctx->dP, ctx->q, ctx->mask, ctx->cellinfo, ctx->gcsx, ctx->gcsy, ctx->ring, ctx->clk,
+      ctx->P, ctx->q, ctx->mask, ctx->cellinfo, ctx->gcsx, ctx->gcsy, ctx->ring, ctx->clk,
       scratch);
   ctx->launches += 1;
   return cudaGetLastError();
@@ -1917,7 +1917,7 @@ extern "C" int imex_gpu_timestep_noalloc(ImexCtx* ctx, double* dt) {
     default: e = launch_cfl_tiles<4>(ctx, scratch); break;
   }
   CK(e);
-  k_cfl_fold<<<1, 1024, 0, ctx->stream>>>(ctx->dP, scratch, n_tiles);
+  k_cfl_fold<<<1, 1024, 0, ctx->stream>>>(ctx->P, scratch, n_tiles);
   ctx->launches += 1;
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(dt, scratch + n_tiles, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));

@@ -87,12 +87,12 @@ __device__ const RingCell* find_ring(const RingCell* ring, int n, long long idx)
 
 // ================================================================= k_mask
 // check_solve(.FALSE.) for n_RK = 2.
-__global__ void __launch_bounds__(256) k_mask(const DevParams* __restrict__ Pp, const double* __restrict__ q1,
+__global__ void __launch_bounds__(256) k_mask(const __grid_constant__ DevParams Pp, const double* __restrict__ q1,
                                               const double* __restrict__ release_time,
                                               const uint8_t* __restrict__ cellinfo,
                                               const DevClock* clk, uint8_t* __restrict__ mask,
                                               DevClock* clkw, int solve_all) {
-  const DevParams& P = *Pp;
+  const DevParams& P = Pp;
   __shared__ uint8_t s0[SH][SW];
   __shared__ uint8_t s1[SH][SW];
   const int j0 = blockIdx.x * TX, k0 = blockIdx.y * TY;
@@ -483,14 +483,14 @@ struct FluxShared {
 
 template <int NS>
 __global__ void __launch_bounds__(FLUX_THREADS, IMEX_FLUX_MINB)
-    k_flux(const DevParams* __restrict__ Pp, const double* __restrict__ q, const uint8_t* __restrict__ mask,
+    k_flux(const __grid_constant__ DevParams Pp, const double* __restrict__ q, const uint8_t* __restrict__ mask,
            const uint8_t* __restrict__ cellinfo, const double* __restrict__ Bx,
            const double* __restrict__ By, const double* __restrict__ Bxx,
            const double* __restrict__ Bxy, const double* __restrict__ Byy,
            const double* __restrict__ gc, const double* __restrict__ dgc,
            const double* __restrict__ gcsx, const double* __restrict__ gcsy,
            const RingCell* __restrict__ ring, DevClock* clk, double* __restrict__ X) {
-  const DevParams& P = *Pp;
+  const DevParams& P = Pp;
   constexpr int NV = 4 + NS, NP = 6 + NS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   FluxShared<NS>& S = *reinterpret_cast<FluxShared<NS>*>(smem_raw);
@@ -1257,13 +1257,13 @@ __device__ __forceinline__ int newton_plain(const DevParams& P, const NewtonWork
 
 template <int NS>
 __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
-    k_stage2_first(const DevParams* __restrict__ Pp, const double* __restrict__ q,
+    k_stage2_first(const __grid_constant__ DevParams Pp, const double* __restrict__ q,
                    const double* __restrict__ X, const uint8_t* __restrict__ mask,
                    const double* __restrict__ Bx, const double* __restrict__ By,
                    const double* __restrict__ Bxx, const double* __restrict__ Bxy,
                    const double* __restrict__ Byy, const double* __restrict__ gc, NewtonWork W,
                    DevClock* clk) {
-  const DevParams& P = *Pp;
+  const DevParams& P = Pp;
   constexpr int NV = 4 + NS, NP = 6 + NS;
   const int nx = P.nx;
   const long long ncell = (long long)nx * P.ny;
@@ -1387,10 +1387,10 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
 // One Newton iteration (nl_iter = 2 or 3) for the cells of list `in`.
 template <int NS>
 __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
-    k_stage2_iter(const DevParams* __restrict__ Pp, const double* __restrict__ q,
+    k_stage2_iter(const __grid_constant__ DevParams Pp, const double* __restrict__ q,
                   const double* __restrict__ Bx, const double* __restrict__ By, NewtonWork W,
                   DevClock* clk, int nl_iter) {
-  const DevParams& P = *Pp;
+  const DevParams& P = Pp;
   constexpr int NV = 4 + NS;
   const size_t N = (size_t)P.plane;
   const double dt = clk->dt;
@@ -1456,10 +1456,10 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
 // Iterations 4..100 for the cells of list 2.
 template <int NS>
 __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
-    k_stage2_tail(const DevParams* __restrict__ Pp, const double* __restrict__ q,
+    k_stage2_tail(const __grid_constant__ DevParams Pp, const double* __restrict__ q,
                   const double* __restrict__ Bx, const double* __restrict__ By, NewtonWork W,
                   DevClock* clk) {
-  const DevParams& P = *Pp;
+  const DevParams& P = Pp;
   constexpr int NV = 4 + NS;
   const size_t N = (size_t)P.plane;
   const double dt = clk->dt;
@@ -1517,10 +1517,10 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
 // 16 cells per warp through the tensor-core forward pass.
 template <int NS>
 __global__ void __launch_bounds__(32 * mlp::WARPS)
-    k_warm_predict(const DevParams* __restrict__ Pp, NewtonWork W, DevClock* clk,
+    k_warm_predict(const __grid_constant__ DevParams Pp, NewtonWork W, DevClock* clk,
                    const __nv_bfloat16* __restrict__ gW, const float* __restrict__ gP,
                    WarmNorm nrm) {
-  const DevParams& P = *Pp;
+  const DevParams& P = Pp;
   const size_t N = (size_t)P.plane;
   extern __shared__ __align__(16) unsigned char smem[];
   __nv_bfloat16* sW = reinterpret_cast<__nv_bfloat16*>(smem);
@@ -1560,10 +1560,10 @@ __global__ void __launch_bounds__(32 * mlp::WARPS)
 // k_stage2_first.
 template <int NS>
 __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
-    k_stage2_wstart(const DevParams* __restrict__ Pp, const double* __restrict__ q,
+    k_stage2_wstart(const __grid_constant__ DevParams Pp, const double* __restrict__ q,
                     const double* __restrict__ Bx, const double* __restrict__ By, NewtonWork W,
                     DevClock* clk) {
-  const DevParams& P = *Pp;
+  const DevParams& P = Pp;
   constexpr int NV = 4 + NS;
   const size_t N = (size_t)P.plane;
   const double dt = clk->dt;
@@ -1619,10 +1619,10 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
 // Warm starts that failed, redone with the plain start (q_si).
 template <int NS>
 __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
-    k_stage2_fallback(const DevParams* __restrict__ Pp, const double* __restrict__ q,
+    k_stage2_fallback(const __grid_constant__ DevParams Pp, const double* __restrict__ q,
                       const double* __restrict__ Bx, const double* __restrict__ By,
                       NewtonWork W, DevClock* clk) {
-  const DevParams& P = *Pp;
+  const DevParams& P = Pp;
   constexpr int NV = 4 + NS;
   const size_t N = (size_t)P.plane;
   const double dt = clk->dt;
@@ -1652,10 +1652,10 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
 // the step, so that successive steps sample different cells).
 template <int NS>
 __global__ void __launch_bounds__(128)
-    k_harvest(const DevParams* __restrict__ Pp, const double* __restrict__ q,
+    k_harvest(const __grid_constant__ DevParams Pp, const double* __restrict__ q,
               const double* __restrict__ Bx, const double* __restrict__ By, NewtonWork W,
               DevClock* clk) {
-  const DevParams& P = *Pp;
+  const DevParams& P = Pp;
   constexpr int NV = 4 + NS;
   const int nx = P.nx;
   const long long ncell = (long long)nx * P.ny;
@@ -1710,10 +1710,10 @@ __global__ void __launch_bounds__(128)
 // (src/solver_2d.f90:1339-1626).
 template <int NS>
 __global__ void __launch_bounds__(STAGE2_THREADS)
-    k_stage2_post(const DevParams* __restrict__ Pp, double* __restrict__ q,
+    k_stage2_post(const __grid_constant__ DevParams Pp, double* __restrict__ q,
                   const uint8_t* __restrict__ mask, const uint8_t* __restrict__ cellinfo,
                   NewtonWork W, DevClock* clk) {
-  const DevParams& P = *Pp;
+  const DevParams& P = Pp;
   constexpr int NV = 4 + NS, NP = 6 + NS;
   const int nx = P.nx, ny = P.ny;
   const long long ncell = (long long)nx * ny;
@@ -1799,11 +1799,11 @@ __global__ void __launch_bounds__(STAGE2_THREADS)
 // Stand-alone erosion/deposition pass (imex_gpu_erosion_deposition).
 template <int NS>
 __global__ void __launch_bounds__(128, IMEX_EROSION_MINB)
-    k_erosion(const DevParams* __restrict__ Pp, double* __restrict__ q, const uint8_t* __restrict__ mask,
+    k_erosion(const __grid_constant__ DevParams Pp, double* __restrict__ q, const uint8_t* __restrict__ mask,
               const double* __restrict__ Bx, const double* __restrict__ By,
               double* __restrict__ erodible, double* __restrict__ deposit,
               double* __restrict__ erosion, double* __restrict__ Bcent, DevClock* clk) {
-  const DevParams& P = *Pp;
+  const DevParams& P = Pp;
   constexpr int NV = 4 + NS;
   const int nx = P.nx;
   const long long ncell = (long long)nx * P.ny;
@@ -1916,9 +1916,9 @@ __global__ void k_soa_to_aos(const double* __restrict__ soa, double* __restrict_
 
 // qp planes for imex_gpu_get_state (driver's post-step convention).
 template <int NS>
-__global__ void k_qp_out(const DevParams* __restrict__ Pp, const double* __restrict__ q, double* __restrict__ qp_aos,
+__global__ void k_qp_out(const __grid_constant__ DevParams Pp, const double* __restrict__ q, double* __restrict__ qp_aos,
                          const uint8_t* __restrict__ cellinfo) {
-  const DevParams& P = *Pp;
+  const DevParams& P = Pp;
   constexpr int NV = 4 + NS, NP = 6 + NS;
   long long n = (long long)P.nx * P.ny;
   for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < n;
@@ -1942,10 +1942,10 @@ __global__ void k_qp_out(const DevParams* __restrict__ Pp, const double* __restr
 // in the border takes the stencil of its nearest interior cell, which is
 // what the reference's copies leave there.
 __global__ void __launch_bounds__(256)
-    k_topo_geom(const DevParams* __restrict__ Pp, const double* __restrict__ B,
+    k_topo_geom(const __grid_constant__ DevParams Pp, const double* __restrict__ B,
                 double* __restrict__ Bx, double* __restrict__ By, double* __restrict__ Bxx,
                 double* __restrict__ Bxy, double* __restrict__ Byy) {
-  const DevParams& P = *Pp;
+  const DevParams& P = Pp;
   const int nx = P.nx, ny = P.ny;
   const long long n = (long long)nx * ny;
   const double c1[5] = {-2.0, -1.0, 0.0, 1.0, 2.0};
@@ -1989,11 +1989,11 @@ __device__ __forceinline__ double topo_gc(double bx, double by) {
 }
 
 __global__ void __launch_bounds__(256)
-    k_topo_gc(const DevParams* __restrict__ Pp, const double* __restrict__ Bx,
+    k_topo_gc(const __grid_constant__ DevParams Pp, const double* __restrict__ Bx,
               const double* __restrict__ By, const double* __restrict__ Bxx,
               const double* __restrict__ Bxy, double* __restrict__ gc, double* __restrict__ dgc,
               double* __restrict__ gcsx, double* __restrict__ gcsy) {
-  const DevParams& P = *Pp;
+  const DevParams& P = Pp;
   const int nx = P.nx, ny = P.ny;
   const long long ncell = (long long)nx * ny, nsx = (long long)(nx + 1) * ny,
                   nsy = (long long)nx * (ny + 1);
@@ -2055,9 +2055,9 @@ struct PostPlanes {
 
 template <int NS>
 __global__ void __launch_bounds__(128)
-    k_post_sweep(const DevParams* __restrict__ Pp, const double* __restrict__ q,
+    k_post_sweep(const __grid_constant__ DevParams Pp, const double* __restrict__ q,
                  const uint8_t* __restrict__ mask, PostPlanes W, PostLevels L, int init) {
-  const DevParams& P = *Pp;
+  const DevParams& P = Pp;
   constexpr int NV = 4 + NS, NP = 6 + NS;
   const long long ncell = (long long)P.nx * P.ny;
   const size_t N = (size_t)P.plane;
@@ -2110,9 +2110,9 @@ __global__ void __launch_bounds__(128)
 constexpr int DIAG_THREADS = 256;
 template <int NS>
 __global__ void __launch_bounds__(DIAG_THREADS)
-    k_post_diag(const DevParams* __restrict__ Pp, const double* __restrict__ q,
+    k_post_diag(const __grid_constant__ DevParams Pp, const double* __restrict__ q,
                 const double* __restrict__ qp_h, double* __restrict__ part) {
-  const DevParams& P = *Pp;
+  const DevParams& P = Pp;
   const long long ncell = (long long)P.nx * P.ny;
   const size_t N = (size_t)P.plane;
   double a[4] = {0.0, 0.0, 0.0, 0.0};
@@ -2152,9 +2152,9 @@ __global__ void k_post_diag_fold(const double* __restrict__ part, int nblocks,
 }
 
 // solve_mask_x / solve_mask_y from solve_mask (src/solver_2d.f90:779-808).
-__global__ void k_masks_xy(const DevParams* __restrict__ Pp, const uint8_t* __restrict__ mask, int8_t* mx,
+__global__ void k_masks_xy(const __grid_constant__ DevParams Pp, const uint8_t* __restrict__ mask, int8_t* mx,
                            int8_t* my) {
-  const DevParams& P = *Pp;
+  const DevParams& P = Pp;
   const int nx = P.nx, ny = P.ny;
   long long nX = (long long)(nx + 1) * ny, nY = (long long)nx * (ny + 1);
   for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < nX + nY;
