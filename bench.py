@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--ens-steps", type=int, default=1000)
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-setup", action="store_true")
     ap.add_argument("--learned-pairs", type=int, default=10_000_000)
     ap.add_argument("--learned-n", type=int, default=1024, help="side of the comparison grid")
     return ap.parse_args()
@@ -213,6 +214,72 @@ def run_ensemble(args):
             "data": "synthetic (seeded sampler: side U{256..1024}, bump height U[5,50] m, "
                     "sigma U[50,300] m, mfr logU[1e6,1e8] kg/s, T U[600,1200] K, "
                     "d logU[1e-5,1e-3] m)"}
+
+
+def run_setup(args):
+    """Set-up on the device (DEM sampling, cell fractions, restart regridding):
+    kernel and end-to-end times at the benchmark's grid size against the CPU
+    oracle on bounded samples of the same routines."""
+    import numpy as np
+    from imex_sflow2d_v2_b200 import configs
+    from imex_sflow2d_v2_b200 import grid_setup as GS
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    n, cs = args.n, 10.0
+    out = {}
+    # DEM of n+2 nodes at the grid's spacing, nodes half a cell west/south of
+    # the cell centres (the reference's node-centred rasters)
+    z = configs.fractal_dem(n + 2, cs, 0.8, 800.0, 15.0, 20261203)
+    dem = GS.Raster(n + 2, n + 2, -cs, -cs, cs, -9999.0, z)
+    GS.init_grid_topography(dem, 64, 64, 0.0, 0.0, cs, check=False)      # warm-up
+    t = {}
+    t0 = time.perf_counter()
+    GS.init_grid_topography(dem, n, n, 0.0, 0.0, cs, check=False, timing=t)
+    e2e = time.perf_counter() - t0
+    m = min(n, 1024)
+    t0 = time.perf_counter()
+    O.setup_dem(z[:m + 2, :m + 2], -cs, -cs, cs, -9999.0, m, m, 0.0, 0.0, cs)
+    cpu = time.perf_counter() - t0
+    out["dem"] = {"cells": n * n, "kernel_ms": t["kernel_ms"], "e2e_ms": e2e * 1e3,
+                  "cells_per_s": n * n / (t["kernel_ms"] * 1e-3),
+                  "e2e_cells_per_s": n * n / e2e,
+                  "cpu_cells_per_s": m * m / cpu, "cpu_sample": "%dx%d grid, 1 thread" % (m, m)}
+    # a collapse of radius n/8 cells at the domain centre
+    r = cs * n / 8
+    c0 = cs * n / 2
+    t = {}
+    t0 = time.perf_counter()
+    f = GS.compute_cell_fract(n, n, 0.0, 0.0, cs, c0, c0, r, 0.7 * r, 30.0, timing=t)
+    e2e = time.perf_counter() - t0
+    cand = int(np.count_nonzero(f)) or 1
+    rc_ = cs * 16
+    t0 = time.perf_counter()
+    fc = O.cell_fract(64, 64, 0.0, 0.0, cs, 320.0, 320.0, rc_, 0.7 * rc_, 30.0)
+    cpu = time.perf_counter() - t0
+    cand_cpu = int(np.count_nonzero(fc)) or 1
+    out["cell_fract"] = {"grid": [n, n], "radius_m": r, "cells_inside": cand,
+                         "kernel_ms": t["kernel_ms"], "e2e_ms": e2e * 1e3,
+                         "subgrid_points_per_s": cand * 40000 / (t["kernel_ms"] * 1e-3),
+                         "cpu_subgrid_points_per_s": cand_cpu * 40000 / cpu,
+                         "cpu_sample": "radius 160 m on a 64x64 grid, OpenMP %d threads"
+                                       % (os.cpu_count() or 1)}
+    # restart raster at 2.5x the grid's resolution over the whole domain
+    nr = int(n * 1.25)
+    fin = np.asfortranarray(np.abs(z[:min(nr, n + 2), :min(nr, n + 2)]) * 1e-3)
+    ras = GS.Raster(fin.shape[0], fin.shape[1], 0.0, 0.0, cs * 0.8, -9999.0, fin)
+    t = {}
+    t0 = time.perf_counter()
+    GS.regrid_scalar(ras, n, n, 0.0, 0.0, cs, timing=t)
+    e2e = time.perf_counter() - t0
+    m = min(n, 512)
+    t0 = time.perf_counter()
+    O.regrid(fin[:int(m * 1.25) + 2, :int(m * 1.25) + 2], 0.0, 0.0, cs * 0.8, -9999.0, m, m,
+             0.0, 0.0, cs)
+    cpu = time.perf_counter() - t0
+    out["regrid"] = {"cells": n * n, "raster": list(fin.shape), "kernel_ms": t["kernel_ms"],
+                     "e2e_ms": e2e * 1e3, "cells_per_s": n * n / (t["kernel_ms"] * 1e-3),
+                     "cpu_cells_per_s": m * m / cpu, "cpu_sample": "%dx%d grid, 1 thread" % (m, m)}
+    return out
 
 
 def run_learned(args, g, p):
@@ -425,6 +492,9 @@ def main():
     ensemble = None
     if rank == 0 and world == 1 and not args.no_ensemble:
         ensemble = run_ensemble(args)
+    setup = None
+    if rank == 0 and world == 1 and not args.no_setup:
+        setup = run_setup(args)
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(args)
@@ -456,6 +526,7 @@ def main():
             "errors": int(s1.error_mask),
             "ensemble": ensemble,
             "learned_vs_plain": learned,
+            "setup": setup,
         }
         print(json.dumps(line), flush=True)
     g.close()

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -16,6 +17,7 @@
 #include "../../include/imex_gpu.h"
 #include "imex_kernels.cuh"
 #include "imex_mlp.cuh"
+#include "imex_setup.cuh"
 
 using namespace imex;
 
@@ -1924,3 +1926,230 @@ extern "C" int imex_gpu_timestep_noalloc(ImexCtx* ctx, double* dt) {
   CK(cudaStreamSynchronize(ctx->stream));
   return IMEX_OK;
 }
+
+// ===================================================== set-up on the device
+namespace {
+
+thread_local std::string g_setup_error;
+
+int setup_fail(int code, const std::string& msg) {
+  g_setup_error = msg;
+  return code;
+}
+#define CKS(call)                                                             \
+  do {                                                                        \
+    cudaError_t e_ = (call);                                                  \
+    if (e_ != cudaSuccess)                                                    \
+      return setup_fail(IMEX_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// Device buffers of one set-up call, freed on every return path.
+struct SetupBufs {
+  std::vector<void*> p;
+  ~SetupBufs() {
+    for (void* b : p) cudaFree(b);
+  }
+  template <class T>
+  cudaError_t alloc(T** out, size_t n) {
+    cudaError_t e = cudaMalloc((void**)out, std::max<size_t>(n, 1) * sizeof(T));
+    if (e == cudaSuccess) p.push_back(*out);
+    return e;
+  }
+};
+
+// Grid spacing as init_grid: cell_size, or 1 along an axis of one cell
+// (src/geometry_2d.f90:250-266).
+SetupGrid setup_grid(int nx, int ny, double x0, double y0, double cell_size) {
+  SetupGrid G;
+  G.nx = nx;
+  G.ny = ny;
+  G.x0 = x0;
+  G.y0 = y0;
+  G.dx = nx > 1 ? cell_size : 1.0;
+  G.dy = ny > 1 ? cell_size : 1.0;
+  return G;
+}
+
+int grid_blocks(long long n, int threads) {
+  return (int)std::max<long long>(1, std::min<long long>((n + threads - 1) / threads, 148LL * 64));
+}
+
+struct EvTimer {
+  cudaEvent_t a = nullptr, b = nullptr;
+  ~EvTimer() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+const char* imex_setup_last_error(void) { return g_setup_error.c_str(); }
+
+int imex_setup_dem(int device, int ncols, int nrows, double xllcorner, double yllcorner,
+                   double cellsize, double nodata, const double* z, int nx, int ny, double x0,
+                   double y0, double cell_size, double* B_cent, int8_t* B_nodata,
+                   float* kernel_ms) {
+  g_setup_error.clear();
+  if (!z || !B_cent || !B_nodata || ncols < 1 || nrows < 1 || nx < 1 || ny < 1)
+    return setup_fail(IMEX_EINVAL, "imex_setup_dem: empty DEM or grid, or NULL array");
+  if (ncols == 1 && nrows == 1)
+    return setup_fail(IMEX_EINVAL, "imex_setup_dem: a DEM of one node cannot be interpolated");
+  if (device >= 0) CKS(cudaSetDevice(device));
+  // node coordinates: xllcorner + (j - 0.5)*cellsize (src/inpout_2d.f90:3579-3589)
+  std::vector<double> x1(ncols), y1(nrows);
+  for (int j = 1; j <= ncols; ++j) x1[j - 1] = xllcorner + ((double)j - 0.5) * cellsize;
+  for (int k = 1; k <= nrows; ++k) y1[k - 1] = yllcorner + ((double)k - 0.5) * cellsize;
+  const size_t nz = (size_t)ncols * nrows, nc = (size_t)nx * ny;
+  SetupBufs B;
+  double *dx1, *dy1, *dz, *dB;
+  int8_t* dN;
+  int* derr;
+  CKS(B.alloc(&dx1, ncols));
+  CKS(B.alloc(&dy1, nrows));
+  CKS(B.alloc(&dz, nz));
+  CKS(B.alloc(&dB, nc));
+  CKS(B.alloc(&dN, nc));
+  CKS(B.alloc(&derr, 1));
+  CKS(cudaMemcpy(dx1, x1.data(), ncols * sizeof(double), cudaMemcpyHostToDevice));
+  CKS(cudaMemcpy(dy1, y1.data(), nrows * sizeof(double), cudaMemcpyHostToDevice));
+  CKS(cudaMemcpy(dz, z, nz * sizeof(double), cudaMemcpyHostToDevice));
+  CKS(cudaMemset(derr, 0, sizeof(int)));
+  const SetupGrid G = setup_grid(nx, ny, x0, y0, cell_size);
+  DemView D{ncols, nrows, dx1, dy1, dz, nodata};
+  EvTimer t;
+  CKS(cudaEventCreate(&t.a));
+  CKS(cudaEventCreate(&t.b));
+  CKS(cudaEventRecord(t.a));
+  k_dem_to_grid<<<grid_blocks((long long)nc, 256), 256>>>(G, D, dB, dN, derr);
+  CKS(cudaGetLastError());
+  CKS(cudaEventRecord(t.b));
+  CKS(cudaEventSynchronize(t.b));
+  if (kernel_ms) CKS(cudaEventElapsedTime(kernel_ms, t.a, t.b));
+  int err = 0;
+  CKS(cudaMemcpy(&err, derr, sizeof(int), cudaMemcpyDeviceToHost));
+  CKS(cudaMemcpy(B_cent, dB, nc * sizeof(double), cudaMemcpyDeviceToHost));
+  CKS(cudaMemcpy(B_nodata, dN, nc, cudaMemcpyDeviceToHost));
+  if (err & SETUP_ERR_NONFINITE)
+    return setup_fail(IMEX_EINVAL, "imex_setup_dem: non-finite DEM or grid coordinates");
+  if (err & SETUP_ERR_OUTSIDE)
+    return setup_fail(IMEX_EINVAL,
+                      "imex_setup_dem: cell centres west or south of the DEM's first node");
+  return IMEX_OK;
+}
+
+int imex_setup_cell_fract(int device, int nx, int ny, double x0, double y0, double cell_size,
+                          double xs, double ys, double rs, double r2s, double angle_deg,
+                          double* cell_fract, float* kernel_ms) {
+  g_setup_error.clear();
+  if (!cell_fract || nx < 1 || ny < 1)
+    return setup_fail(IMEX_EINVAL, "imex_setup_cell_fract: empty grid or NULL array");
+  if (device >= 0) CKS(cudaSetDevice(device));
+  const SetupGrid G = setup_grid(nx, ny, x0, y0, cell_size);
+  // ang_rad = angles/180*ATAN(1)*4 with the host's libm (src/geometry_2d.f90:1696)
+  const double ang_rad = ((angle_deg / 180.0) * std::atan(1.0)) * 4.0;
+  const double ca = std::cos(ang_rad), sa = std::sin(ang_rad);
+  const double R = (rs > r2s) ? rs : r2s;
+  // cells whose box meets the bounding square (the test of :1727-1730)
+  auto x_stag = [&](int J) { return G.x0 + (double)(J - 1) * G.dx; };
+  auto y_stag = [&](int K) { return G.y0 + (double)(K - 1) * G.dy; };
+  int jlo = -1, jhi = -2, klo = -1, khi = -2;
+  for (int j = 1; j <= nx; ++j)
+    if (!(x_stag(j + 1) < (xs - R)) && !(x_stag(j) > (xs + R))) {
+      if (jlo < 0) jlo = j;
+      jhi = j;
+    }
+  for (int k = 1; k <= ny; ++k)
+    if (!(y_stag(k + 1) < (ys - R)) && !(y_stag(k) > (ys + R))) {
+      if (klo < 0) klo = k;
+      khi = k;
+    }
+  // subgrid offsets ((2h-1)/(2n) - 1/2)*dx (src/geometry_2d.f90:1711-1722)
+  std::vector<double> xsub(CF_POINTS), ysub(CF_POINTS);
+  for (int h = 1; h <= CF_POINTS; ++h) {
+    const double u = (2.0 * (double)h - 1.0) / (2.0 * (double)CF_POINTS);
+    xsub[h - 1] = (u - 0.5) * G.dx;
+    ysub[h - 1] = (u - 0.5) * G.dy;
+  }
+  const size_t nc = (size_t)nx * ny;
+  SetupBufs B;
+  double *dxs, *dys, *dout;
+  CKS(B.alloc(&dxs, CF_POINTS));
+  CKS(B.alloc(&dys, CF_POINTS));
+  CKS(B.alloc(&dout, nc));
+  CKS(cudaMemcpy(dxs, xsub.data(), CF_POINTS * sizeof(double), cudaMemcpyHostToDevice));
+  CKS(cudaMemcpy(dys, ysub.data(), CF_POINTS * sizeof(double), cudaMemcpyHostToDevice));
+  CKS(cudaMemset(dout, 0, nc * sizeof(double)));
+  EvTimer t;
+  CKS(cudaEventCreate(&t.a));
+  CKS(cudaEventCreate(&t.b));
+  CKS(cudaEventRecord(t.a));
+  if (jlo > 0 && klo > 0) {
+    CellFractArgs A;
+    A.G = G;
+    A.j_lo = jlo - 1;
+    A.k_lo = klo - 1;
+    A.n_j = jhi - jlo + 1;
+    A.n_k = khi - klo + 1;
+    A.xs = xs;
+    A.ys = ys;
+    A.rs2 = rs * rs;
+    A.r2s2 = r2s * r2s;
+    A.cos_a = ca;
+    A.sin_a = sa;
+    const long long ncand = (long long)A.n_j * A.n_k;
+    const int blocks = (int)std::min<long long>(ncand, 148LL * 16);
+    k_cell_fract<<<blocks, CF_THREADS>>>(A, dxs, dys, dout);
+    CKS(cudaGetLastError());
+  }
+  CKS(cudaEventRecord(t.b));
+  CKS(cudaEventSynchronize(t.b));
+  if (kernel_ms) CKS(cudaEventElapsedTime(kernel_ms, t.a, t.b));
+  CKS(cudaMemcpy(cell_fract, dout, nc * sizeof(double), cudaMemcpyDeviceToHost));
+  return IMEX_OK;
+}
+
+int imex_setup_regrid(int device, int ncols, int nrows, double xllcorner, double yllcorner,
+                      double cellsize, double nodata, const double* fin, int nx, int ny,
+                      double x0, double y0, double cell_size, double* fout, float* kernel_ms) {
+  g_setup_error.clear();
+  if (!fin || !fout || ncols < 1 || nrows < 1 || nx < 1 || ny < 1)
+    return setup_fail(IMEX_EINVAL, "imex_setup_regrid: empty raster or grid, or NULL array");
+  if (device >= 0) CKS(cudaSetDevice(device));
+  // raster edges xllcorner + (j-1)*cellsize, j = 1..ncols+1 (src/inpout_2d.f90:5203-5213)
+  std::vector<double> xin(ncols + 1), yin(nrows + 1);
+  for (int j = 1; j <= ncols + 1; ++j) xin[j - 1] = xllcorner + (double)(j - 1) * cellsize;
+  for (int k = 1; k <= nrows + 1; ++k) yin[k - 1] = yllcorner + (double)(k - 1) * cellsize;
+  const size_t nr = (size_t)ncols * nrows, nc = (size_t)nx * ny;
+  SetupBufs B;
+  double *dxin, *dyin, *dfin, *dout;
+  int* derr;
+  CKS(B.alloc(&dxin, ncols + 1));
+  CKS(B.alloc(&dyin, nrows + 1));
+  CKS(B.alloc(&dfin, nr));
+  CKS(B.alloc(&dout, nc));
+  CKS(B.alloc(&derr, 1));
+  CKS(cudaMemcpy(dxin, xin.data(), (ncols + 1) * sizeof(double), cudaMemcpyHostToDevice));
+  CKS(cudaMemcpy(dyin, yin.data(), (nrows + 1) * sizeof(double), cudaMemcpyHostToDevice));
+  CKS(cudaMemcpy(dfin, fin, nr * sizeof(double), cudaMemcpyHostToDevice));
+  CKS(cudaMemset(derr, 0, sizeof(int)));
+  RegridArgs A{nx, ny, x0, y0, cell_size, ncols, nrows, nodata};
+  EvTimer t;
+  CKS(cudaEventCreate(&t.a));
+  CKS(cudaEventCreate(&t.b));
+  CKS(cudaEventRecord(t.a));
+  k_regrid<<<grid_blocks((long long)nc, 256), 256>>>(A, dxin, dyin, dfin, dout, derr);
+  CKS(cudaGetLastError());
+  CKS(cudaEventRecord(t.b));
+  CKS(cudaEventSynchronize(t.b));
+  if (kernel_ms) CKS(cudaEventElapsedTime(kernel_ms, t.a, t.b));
+  int err = 0;
+  CKS(cudaMemcpy(&err, derr, sizeof(int), cudaMemcpyDeviceToHost));
+  CKS(cudaMemcpy(fout, dout, nc * sizeof(double), cudaMemcpyDeviceToHost));
+  if (err) return setup_fail(IMEX_EINVAL, "imex_setup_regrid: non-finite raster or grid coordinates");
+  return IMEX_OK;
+}
+
+}  // extern "C"

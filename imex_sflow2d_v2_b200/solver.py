@@ -66,6 +66,14 @@ def load_library(path=LIB_PATH):
         "imex_gpu_kernel_times": ([vp, dp, i64p, C.c_int], C.c_int),
         "imex_gpu_measure_fp64_peak": ([C.c_int, dp], C.c_int),
         "imex_gpu_build_info": ([], C.c_char_p),
+        "imex_setup_dem": ([C.c_int, C.c_int, C.c_int] + [C.c_double] * 4 + [dp, C.c_int, C.c_int]
+                           + [C.c_double] * 3 + [dp, i8p, C.POINTER(C.c_float)], C.c_int),
+        "imex_setup_cell_fract": ([C.c_int, C.c_int, C.c_int] + [C.c_double] * 8
+                                  + [dp, C.POINTER(C.c_float)], C.c_int),
+        "imex_setup_regrid": ([C.c_int, C.c_int, C.c_int] + [C.c_double] * 4
+                              + [dp, C.c_int, C.c_int] + [C.c_double] * 3
+                              + [dp, C.POINTER(C.c_float)], C.c_int),
+        "imex_setup_last_error": ([], C.c_char_p),
         "imex_gpu_post_init": ([vp, C.c_int, dp, C.c_int, dp], C.c_int),
         "imex_gpu_post_step": ([vp, C.POINTER(ImexPostDiag)], C.c_int),
         "imex_gpu_post_diag": ([vp, C.POINTER(ImexPostDiag)], C.c_int),

@@ -353,6 +353,49 @@ int imex_gpu_ensemble_tuning(ImexEnsemble* ens, int* k_streams, int* n_tried, in
                              float* tried_ms, int cap);
 const char* imex_gpu_ensemble_last_error(ImexEnsemble* ens);
 
+/*
+ * Set-up on the device (no context needed).  Inputs and outputs are host
+ * arrays in the reference's column-major layouts; each call copies its
+ * inputs to `device` (< 0: the current one), runs one kernel and copies the
+ * result back.  *kernel_ms (may be NULL) receives the kernel's device time.
+ * Errors: IMEX_EINVAL with a message in imex_setup_last_error().
+ *
+ * imex_setup_dem replaces init_grid's DEM sampling (src/geometry_2d.f90:
+ * 320-342): B_nodata = interp_2d_nodata (:1242-1296) on the heights as read,
+ * B_cent = interp_2d_scalar (:1174-1226) on MAX(0, heights), at the cell
+ * centres of the nx*ny grid with origin (x0, y0) and spacing cell_size (1
+ * along an axis of one cell, :250-266).  z is topography_profile(3,:,:):
+ * (ncols, nrows), row 1 the southernmost; node (j,k) sits at
+ * (xllcorner+(j-0.5)*cellsize, yllcorner+(k-0.5)*cellsize)
+ * (src/inpout_2d.f90:3572-3605).  A cell centre west or south of the first
+ * node (where the reference would index outside the DEM) is an error.
+ *
+ * imex_setup_cell_fract replaces compute_cell_fract (src/geometry_2d.f90:
+ * 1678-1773): the share of each cell's 200x200 subgrid points inside the
+ * ellipse of centre (xs, ys), semi-axes rs, r2s, rotated by angle_deg, as
+ * REAL(count)/40000 in single precision; 0 outside the bounding square.
+ * cos/sin of the angle come from the host's libm.
+ *
+ * imex_setup_regrid replaces the restart regridding of read_solution
+ * (src/inpout_2d.f90:5203-5246 with regrid_scalar, src/geometry_2d.f90:
+ * 1491-1534): the area-weighted average of the raster fin (ncols, nrows,
+ * row 1 southernmost, cell edges at xllcorner+(j-1)*cellsize) over each
+ * cell [x0+(j-1)*cell_size, x0+j*cell_size] x [...]; values equal to
+ * nodata count as 0.  The reference's loop bounds are kept (the raster's
+ * last column is never read: ix2 <= ncols).
+ */
+int imex_setup_dem(int device, int ncols, int nrows, double xllcorner, double yllcorner,
+                   double cellsize, double nodata, const double* z, int nx, int ny, double x0,
+                   double y0, double cell_size, double* B_cent, int8_t* B_nodata,
+                   float* kernel_ms);
+int imex_setup_cell_fract(int device, int nx, int ny, double x0, double y0, double cell_size,
+                          double xs, double ys, double rs, double r2s, double angle_deg,
+                          double* cell_fract, float* kernel_ms);
+int imex_setup_regrid(int device, int ncols, int nrows, double xllcorner, double yllcorner,
+                      double cellsize, double nodata, const double* fin, int nx, int ny,
+                      double x0, double y0, double cell_size, double* fout, float* kernel_ms);
+const char* imex_setup_last_error(void);
+
 /* Build information: "sm_100a fmad=0 ..." */
 const char* imex_gpu_build_info(void);
 

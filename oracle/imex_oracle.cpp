@@ -2582,3 +2582,166 @@ extern "C" void oracle_get_topo(OracleCtx* o, double* bx, double* by, double* bx
     if (dgc) dgc[c] = o->dgc_dx[c];
   }
 }
+
+// ---------------------------------------------------------------- set-up
+// Restatements of init_grid's DEM sampling, compute_cell_fract and the
+// restart regridding, loop for loop as the reference writes them.
+
+// init_grid's x_stag/x_comp (src/geometry_2d.f90:250-320) for a grid of n
+// cells: spacing cell_size, or 1 for a single cell.
+static double setup_comp(double o, double d, int J) {   // J 1-based
+  const double a = o + (double)(J - 1) * d, b = o + (double)J * d;
+  return 0.5 * (a + b);
+}
+
+// src/geometry_2d.f90:320-342 with interp_2d_nodata (:1242-1296) and
+// interp_2d_scalar (:1174-1226); node coordinates per src/inpout_2d.f90:
+// 3579-3589.  Returns 0, or 1 when a cell centre lies west/south of the
+// first node (the reference would index outside the DEM), 2 for a
+// non-finite index.
+extern "C" int oracle_setup_dem(int ncols, int nrows, double xll, double yll, double cs,
+                                double nodata, const double* z, int nx, int ny, double x0,
+                                double y0, double cell_size, double* B_cent, int8_t* B_nodata) {
+  const double dx = nx > 1 ? cell_size : 1.0, dy = ny > 1 ? cell_size : 1.0;
+  std::vector<double> x1(ncols), y1(nrows), zc((size_t)ncols * nrows);
+  for (int j = 1; j <= ncols; ++j) x1[j - 1] = xll + ((double)j - 0.5) * cs;
+  for (int k = 1; k <= nrows; ++k) y1[k - 1] = yll + ((double)k - 0.5) * cs;
+  for (size_t i = 0; i < zc.size(); ++i) zc[i] = fmax_f(0.0, z[i]);   // MAX(0, z)
+  auto Z = [&](const double* a, int ix, int iy) { return a[(size_t)(ix - 1) + (size_t)(iy - 1) * ncols]; };
+  int status = 0;
+  for (int k = 1; k <= ny; ++k) {
+    for (int j = 1; j <= nx; ++j) {
+      const double x2 = setup_comp(x0, dx, j), y2 = setup_comp(y0, dy, k);
+      const size_t c = (size_t)(j - 1) + (size_t)(k - 1) * nx;
+      int ix = 1, iy = 1;
+      double ax = 0.0, ay = 0.0;
+      bool ok = true;
+      if (ncols > 1) {
+        const double v = (x2 - x1[0]) / (x1[1] - x1[0]);
+        if (!(v > -1.0e9 && v < 1.0e9)) ok = false;
+        else ix = std::min((int)std::floor(v) + 1, ncols - 1);
+      }
+      if (nrows > 1) {
+        const double v = (y2 - y1[0]) / (y1[1] - y1[0]);
+        if (!(v > -1.0e9 && v < 1.0e9)) ok = false;
+        else iy = std::min((int)std::floor(v) + 1, nrows - 1);
+      }
+      if (!ok || ix < 1 || iy < 1) {
+        status |= ok ? 1 : 2;
+        B_cent[c] = 0.0;
+        B_nodata[c] = 0;
+        continue;
+      }
+      if (ncols > 1) ax = (x1[ix] - x2) / (x1[ix] - x1[ix - 1]);
+      if (nrows > 1) ay = (y1[iy] - y2) / (y1[iy] - y1[iy - 1]);
+      bool nod;
+      double f2;
+      if (ncols == 1) {
+        nod = (Z(z, ix, iy) == nodata) || (Z(z, ix, iy + 1) == nodata);
+        f2 = ay * Z(zc.data(), ix, iy) + (1.0 - ay) * Z(zc.data(), ix, iy + 1);
+      } else if (nrows == 1) {
+        nod = (Z(z, ix, iy) == nodata) || (Z(z, ix + 1, iy) == nodata);
+        f2 = ax * Z(zc.data(), ix, iy) + (1.0 - ax) * Z(zc.data(), ix + 1, iy);
+      } else {
+        nod = (Z(z, ix, iy) == nodata) || (Z(z, ix, iy + 1) == nodata) ||
+              (Z(z, ix + 1, iy) == nodata) || (Z(z, ix + 1, iy + 1) == nodata);
+        f2 = ax * (ay * Z(zc.data(), ix, iy) + (1.0 - ay) * Z(zc.data(), ix, iy + 1)) +
+             (1.0 - ax) * (ay * Z(zc.data(), ix + 1, iy) + (1.0 - ay) * Z(zc.data(), ix + 1, iy + 1));
+      }
+      B_cent[c] = f2;
+      B_nodata[c] = nod ? 1 : 0;
+    }
+  }
+  return status;
+}
+
+// compute_cell_fract (src/geometry_2d.f90:1678-1773): every subgrid point of
+// every cell that meets the bounding square.
+extern "C" void oracle_cell_fract(int nx, int ny, double x0, double y0, double cell_size,
+                                  double xs, double ys, double rs, double r2s, double angle_deg,
+                                  double* cell_fract) {
+  const int n = 200, n2 = n * n;
+  const double dx = nx > 1 ? cell_size : 1.0, dy = ny > 1 ? cell_size : 1.0;
+  const double ang_rad = ((angle_deg / 180.0) * std::atan(1.0)) * 4.0;
+  const double ca = std::cos(ang_rad), sa = std::sin(ang_rad);
+  std::vector<double> xsub(n2), ysub(n2);
+  for (int h = 1; h <= n; ++h) {
+    for (int i = h; i <= n2; i += n) xsub[i - 1] = (double)h;
+    for (int i = (h - 1) * n + 1; i <= h * n; ++i) ysub[i - 1] = (double)h;
+  }
+  for (int i = 0; i < n2; ++i) {
+    xsub[i] = (2.0 * xsub[i] - 1.0) / (2.0 * (double)n);
+    ysub[i] = (2.0 * ysub[i] - 1.0) / (2.0 * (double)n);
+    xsub[i] = (xsub[i] - 0.5) * dx;
+    ysub[i] = (ysub[i] - 0.5) * dy;
+  }
+  const double R = (rs > r2s) ? rs : r2s;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int j = 1; j <= nx; ++j) {
+    const double xsj = x0 + (double)(j - 1) * dx, xsj1 = x0 + (double)j * dx;
+    const double xc = 0.5 * (xsj + xsj1);
+    for (int k = 1; k <= ny; ++k) {
+      const double ysk = y0 + (double)(k - 1) * dy, ysk1 = y0 + (double)k * dy;
+      const double yc = 0.5 * (ysk + ysk1);
+      double& out = cell_fract[(size_t)(j - 1) + (size_t)(k - 1) * nx];
+      if (xsj1 < (xs - R) || xsj > (xs + R) || ysk1 < (ys - R) || ysk > (ys + R)) {
+        out = 0.0;
+        continue;
+      }
+      int cnt = 0;
+      for (int i = 0; i < n2; ++i) {
+        const double X = (xc + xsub[i]) - xs, Y = (yc + ysub[i]) - ys;
+        const double u = X * ca + Y * sa;
+        const double v = -(X * sa) + Y * ca;
+        if ((u * u) / (rs * rs) + (v * v) / (r2s * r2s) <= 1.0) cnt += 1;
+      }
+      out = (double)((float)cnt / (float)n2);
+    }
+  }
+}
+
+// read_solution's regridding of a restart raster (src/inpout_2d.f90:
+// 5190-5246) through regrid_scalar (src/geometry_2d.f90:1491-1534).
+// Returns 0, or 2 for a non-finite index.
+extern "C" int oracle_regrid(int ncols, int nrows, double xll, double yll, double cs,
+                             double nodata, const double* fin_raw, int nx, int ny, double x0,
+                             double y0, double cell_size, double* fout) {
+  std::vector<double> xin(ncols + 1), yin(nrows + 1), fin(fin_raw, fin_raw + (size_t)ncols * nrows);
+  for (auto& v : fin)
+    if (v == nodata) v = 0.0;
+  for (int j = 1; j <= ncols + 1; ++j) xin[j - 1] = xll + (double)(j - 1) * cs;
+  for (int k = 1; k <= nrows + 1; ++k) yin[k - 1] = yll + (double)(k - 1) * cs;
+  const int nXin = ncols, nYin = nrows + 1;
+  const double dXin = xin[1] - xin[0], dYin = yin[1] - yin[0];
+  auto ceil_ok = [](double v, int& o) {
+    if (!(v > -1.0e9 && v < 1.0e9)) return false;
+    o = (int)std::ceil(v);
+    return true;
+  };
+  int status = 0;
+  for (int j = 1; j <= nx; ++j) {
+    const double xl = x0 + (double)(j - 1) * cell_size, xr = x0 + (double)j * cell_size;
+    for (int k = 1; k <= ny; ++k) {
+      const double yl = y0 + (double)(k - 1) * cell_size, yr = y0 + (double)k * cell_size;
+      double& f = fout[(size_t)(j - 1) + (size_t)(k - 1) * nx];
+      int a, b, c, d;
+      if (!ceil_ok((xl - xin[0]) / dXin, a) || !ceil_ok((xr - xin[0]) / dXin, b) ||
+          !ceil_ok((yl - yin[0]) / dYin, c) || !ceil_ok((yr - yin[0]) / dYin, d)) {
+        status |= 2;
+        f = 0.0;
+        continue;
+      }
+      const int ix1 = std::max(1, a), ix2 = std::min(nXin, b + 1);
+      const int iy1 = std::max(1, c), iy2 = std::min(nYin, d + 1);
+      f = 0.0;
+      for (int ix = ix1; ix <= ix2 - 1; ++ix) {
+        const double alfa_x = (fmin_f(xr, xin[ix]) - fmax_f(xl, xin[ix - 1])) / (xr - xl);
+        for (int iy = iy1; iy <= iy2 - 1; ++iy) {
+          const double alfa_y = (fmin_f(yr, yin[iy]) - fmax_f(yl, yin[iy - 1])) / (yr - yl);
+          f = f + alfa_x * alfa_y * fin[(size_t)(ix - 1) + (size_t)(iy - 1) * ncols];
+        }
+      }
+    }
+  }
+  return status;
+}

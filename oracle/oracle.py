@@ -70,6 +70,14 @@ def lib():
         L.oracle_get_post.argtypes = [vp, dp, dp, dp, C.POINTER(C.c_int8)]
         L.oracle_topography_reconstruction.argtypes = [vp]
         L.oracle_get_topo.argtypes = [vp] + [dp] * 7
+        i8p = C.POINTER(C.c_int8)
+        L.oracle_setup_dem.restype = C.c_int
+        L.oracle_setup_dem.argtypes = ([C.c_int, C.c_int] + [C.c_double] * 4 + [dp, C.c_int, C.c_int]
+                                       + [C.c_double] * 3 + [dp, i8p])
+        L.oracle_cell_fract.argtypes = [C.c_int, C.c_int] + [C.c_double] * 8 + [dp]
+        L.oracle_regrid.restype = C.c_int
+        L.oracle_regrid.argtypes = ([C.c_int, C.c_int] + [C.c_double] * 4 + [dp, C.c_int, C.c_int]
+                                    + [C.c_double] * 3 + [dp])
         L.oracle_limit.restype = C.c_double
         L.oracle_limit.argtypes = [C.c_double] * 6 + [C.c_int, C.c_double]
         _LIB = L
@@ -236,3 +244,29 @@ def ipow(x, y):
 
 def limit(v1, v2, v3, z1, z2, z3, limiter, theta=1.0):
     return lib().oracle_limit(v1, v2, v3, z1, z2, z3, int(limiter), float(theta))
+
+
+def setup_dem(z, xll, yll, cellsize, nodata, nx, ny, x0, y0, cell_size):
+    """(B_cent, B_nodata, status) of init_grid's DEM sampling; z is (ncols, nrows)."""
+    z = np.asfortranarray(z, dtype=np.float64)
+    ncols, nrows = z.shape
+    B = np.zeros((nx, ny), dtype=np.float64, order="F")
+    N = np.zeros((nx, ny), dtype=np.int8, order="F")
+    st = lib().oracle_setup_dem(ncols, nrows, xll, yll, cellsize, nodata, _p(z), nx, ny, x0, y0,
+                                cell_size, _p(B), N.ctypes.data_as(C.POINTER(C.c_int8)))
+    return B, N, st
+
+
+def cell_fract(nx, ny, x0, y0, cell_size, xs, ys, rs, r2s, angle):
+    out = np.zeros((nx, ny), dtype=np.float64, order="F")
+    lib().oracle_cell_fract(nx, ny, x0, y0, cell_size, xs, ys, rs, r2s, angle, _p(out))
+    return out
+
+
+def regrid(fin, xll, yll, cellsize, nodata, nx, ny, x0, y0, cell_size):
+    fin = np.asfortranarray(fin, dtype=np.float64)
+    ncols, nrows = fin.shape
+    out = np.zeros((nx, ny), dtype=np.float64, order="F")
+    st = lib().oracle_regrid(ncols, nrows, xll, yll, cellsize, nodata, _p(fin), nx, ny, x0, y0,
+                             cell_size, _p(out))
+    return out, st
