@@ -116,6 +116,12 @@ class ImexStats(C.Structure):
     ]
 
 
+class ImexOutputSpec(C.Structure):
+    _fields_ = [("run_name", C.c_char_p), ("output_idx", C.c_int), ("time", C.c_double),
+                ("cons", C.c_int), ("phys", C.c_int), ("esri", C.c_int), ("max_grid", C.c_int),
+                ("threads", C.c_int)]
+
+
 class ImexPostDiag(C.Structure):
     _fields_ = [("mass", C.c_double), ("volume", C.c_double), ("area", C.c_double),
                 ("solid_mass", C.c_double)]

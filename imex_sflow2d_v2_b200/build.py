@@ -10,7 +10,8 @@ LIB = os.path.join(_HERE, "libimexgpu.so")
 
 def sources():
     return [os.path.join(CSRC, f) for f in ("imex_gpu.cu", "imex_kernels.cuh", "imex_mlp.cuh",
-                                             "imex_device.cuh", "imex_setup.cuh",
+                                             "imex_device.cuh", "imex_setup.cuh", "imex_output.cuh",
+                                             "imex_fortran_fmt.h",
                                              "ipow_tables.h")] + [
         os.path.join(_HERE, "..", "include", "imex_gpu.h")]
 

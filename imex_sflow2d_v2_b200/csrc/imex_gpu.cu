@@ -12,12 +12,15 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/imex_gpu.h"
 #include "imex_kernels.cuh"
 #include "imex_mlp.cuh"
 #include "imex_setup.cuh"
+#include "imex_output.cuh"
+#include "imex_fortran_fmt.h"
 
 using namespace imex;
 
@@ -59,6 +62,17 @@ struct ImexCtx {
   double* nw_guess = nullptr;
   float* h_x = nullptr;
   float* h_y = nullptr;
+  // output_solution writer (imex_gpu_output): device planes, pinned staging,
+  // the event after the staging copies and the host thread that formats
+  std::thread out_thread;
+  bool out_pending = false;
+  int out_status = 0;
+  std::string out_error;
+  double* out_dev = nullptr;
+  size_t out_dev_n = 0;
+  double* out_host = nullptr;
+  size_t out_host_n = 0;
+  cudaEvent_t out_ev = nullptr;
   size_t scratch_bytes = 0;
   bool x_valid = false;          // X holds the fluxes of the current state
   bool exchange = false;         // erosion/deposition planes present
@@ -600,6 +614,10 @@ int imex_gpu_create(const ImexParams* p, const ImexStatic* s, int device, ImexCt
     CK(dalloc(&ctx->release, plane));
     CK(upload_plane(ctx, ctx->release, s->solve_mask_time, 0.0));
   }
+  if (!ctx->exchange && !P.topo_change_flag && s->B_cent) {   // for the output writers
+    CK(dalloc(&ctx->Bcent, plane));
+    CK(upload_plane(ctx, ctx->Bcent, s->B_cent, 0.0));
+  }
   if (ctx->exchange || P.topo_change_flag) {
     const int ns = P.ns;
     CK(dalloc(&ctx->erodible, plane * ns));
@@ -646,6 +664,10 @@ int imex_gpu_destroy(ImexCtx* ctx) {
   if (!ctx) return IMEX_EINVAL;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->out_thread.joinable()) ctx->out_thread.join();
+  if (ctx->out_dev) cudaFree(ctx->out_dev);
+  if (ctx->out_host) cudaFreeHost(ctx->out_host);
+  if (ctx->out_ev) cudaEventDestroy(ctx->out_ev);
   if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
   if (ctx->graph) cudaGraphDestroy(ctx->graph);
   void* bufs[] = {ctx->q, ctx->X, ctx->mask, ctx->cellinfo, ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy,
@@ -2149,6 +2171,398 @@ int imex_setup_regrid(int device, int ncols, int nrows, double xllcorner, double
   CKS(cudaMemcpy(&err, derr, sizeof(int), cudaMemcpyDeviceToHost));
   CKS(cudaMemcpy(fout, dout, nc * sizeof(double), cudaMemcpyDeviceToHost));
   if (err) return setup_fail(IMEX_EINVAL, "imex_setup_regrid: non-finite raster or grid coordinates");
+  return IMEX_OK;
+}
+
+}  // extern "C"
+
+// ===================================================== output_solution writers
+namespace {
+
+// One output_solution call: which files, and where each staged plane sits in
+// the pinned buffer (offsets in units of nx*ny doubles; -1 = not staged).
+struct OutJob {
+  std::string run;
+  int idx = 0, nx = 0, ny = 0, ns = 0, nv = 0, threads = 1;
+  double x0 = 0, y0 = 0, dx = 1, dy = 1, cell_size = 1, porosity = 0;
+  bool cons = false, phys = false, esri = false, maxf = false, first = false;
+  bool erosion = false, settling = false, topo = false;
+  long q = -1, ers_c = -1, erd_c = -1, dep_c = -1, B_c = -1;   // .q_2d family
+  long p2d = -1;                                               // .p_2d columns
+  long esr = -1, dep_e = -1, ers_e = -1, hmax = -1;            // ESRI grids
+  const double* buf = nullptr;
+};
+
+double out_x_comp(const OutJob& J, int j) {   // j 1-based (src/geometry_2d.f90:294-320)
+  return 0.5 * ((J.x0 + (double)(j - 1) * J.dx) + (J.x0 + (double)j * J.dx));
+}
+double out_y_comp(const OutJob& J, int k) {
+  return 0.5 * ((J.y0 + (double)(k - 1) * J.dy) + (J.y0 + (double)k * J.dy));
+}
+
+// Rows k = 1..ny of a column file, formatted by `threads` workers in bands
+// and written in order; each line is x_comp, y_comp and `cols` values.
+// kind 0: E20.12 ('(2e20.12,100(e20.12))'), kind 1: ES15.7E2 ('100ES15.7E2').
+// A list-directed WRITE(u,*) ' ' ends every row and two more end the file.
+bool write_columns(const OutJob& J, const std::string& path, int kind,
+                   const std::vector<const double*>& cols, std::string& err) {
+  FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f) {
+    err = "cannot open " + path;
+    return false;
+  }
+  const size_t n = (size_t)J.nx * J.ny;
+  (void)n;
+  const int T = std::max(1, J.threads);
+  const int band = 16;   // rows per task
+  std::vector<std::string> text(T);
+  bool ok = true;
+  for (int k0 = 1; k0 <= J.ny && ok; k0 += band * T) {
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; ++t) {
+      th.emplace_back([&, t]() {
+        std::string& o = text[t];
+        o.clear();
+        const int ka = k0 + t * band, kb = std::min(J.ny, ka + band - 1);
+        for (int k = ka; k <= kb; ++k) {
+          for (int j = 1; j <= J.nx; ++j) {
+            const size_t c = (size_t)(j - 1) + (size_t)(k - 1) * J.nx;
+            if (kind == 0) {
+              ffmt::E(o, out_x_comp(J, j), 20, 12);
+              ffmt::E(o, out_y_comp(J, k), 20, 12);
+              for (const double* p : cols) ffmt::E(o, p[c], 20, 12);
+            } else {
+              ffmt::ES(o, out_x_comp(J, j), 15, 7, 2);
+              ffmt::ES(o, out_y_comp(J, k), 15, 7, 2);
+              for (const double* p : cols) ffmt::ES(o, p[c], 15, 7, 2);
+            }
+            o.push_back('\n');
+          }
+          o.append("  \n");
+        }
+      });
+    }
+    for (auto& x : th) x.join();
+    for (int t = 0; t < T && ok; ++t)
+      if (!text[t].empty() && std::fwrite(text[t].data(), 1, text[t].size(), f) != text[t].size())
+        ok = false;
+  }
+  if (ok) ok = std::fputs("  \n  \n", f) >= 0;
+  if (std::fclose(f) != 0) ok = false;
+  if (!ok) err = "write failed: " + path;
+  return ok;
+}
+
+// An ESRI grid as output_esri/output_max write it: the six header records
+// ('(A,I5)' / '(A,F15.3)') and rows from north to south in '(2000ES12.3E3)',
+// 2000 values per record.  `val(c)` gives the printed value of cell c.
+template <class F>
+bool write_esri(const OutJob& J, const std::string& path, F val, std::string& err) {
+  FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f) {
+    err = "cannot open " + path;
+    return false;
+  }
+  std::string o;
+  o += "ncols ";
+  ffmt::I(o, J.nx, 5);
+  o += "\nnrows ";
+  ffmt::I(o, J.ny, 5);
+  o += "\nxllcorner ";
+  ffmt::F(o, J.x0, 15, 3);
+  o += "\nyllcorner ";
+  ffmt::F(o, J.y0, 15, 3);
+  o += "\ncellsize ";
+  ffmt::F(o, J.cell_size, 15, 3);
+  o += "\nNODATA_value ";
+  ffmt::I(o, -9999, 5);
+  o += "\n";
+  bool ok = std::fwrite(o.data(), 1, o.size(), f) == o.size();
+  for (int k = J.ny; k >= 1 && ok; --k) {
+    o.clear();
+    for (int j = 1; j <= J.nx; ++j) {
+      ffmt::ES(o, val((size_t)(j - 1) + (size_t)(k - 1) * J.nx), 12, 3, 3);
+      if (j % 2000 == 0 || j == J.nx) o.push_back('\n');
+    }
+    ok = std::fwrite(o.data(), 1, o.size(), f) == o.size();
+  }
+  if (std::fclose(f) != 0) ok = false;
+  if (!ok) err = "write failed: " + path;
+  return ok;
+}
+
+int run_out_job(const OutJob& J, std::string& err) {
+  const size_t n = (size_t)J.nx * J.ny;
+  auto P = [&](long off, int i) { return J.buf + (size_t)(off + i) * n; };
+  const std::string idx = ffmt::lettera(J.idx - 1);
+  if (J.cons) {
+    std::vector<const double*> c;
+    for (int i = 0; i < J.nv; ++i) c.push_back(P(J.q, i));
+    if (!write_columns(J, J.run + "_" + idx + ".q_2d", 0, c, err)) return IMEX_EINVAL;
+    if (J.erosion) {
+      c.clear();
+      for (int i = 0; i < J.ns; ++i) c.push_back(P(J.ers_c, i));
+      if (!write_columns(J, J.run + "_erosion_" + idx + ".q_2d", 0, c, err)) return IMEX_EINVAL;
+      c.clear();
+      for (int i = 0; i < J.ns; ++i) c.push_back(P(J.erd_c, i));
+      if (!write_columns(J, J.run + "_erodible_" + idx + ".q_2d", 0, c, err)) return IMEX_EINVAL;
+    }
+    if (J.settling) {
+      c.clear();
+      for (int i = 0; i < J.ns; ++i) c.push_back(P(J.dep_c, i));
+      if (!write_columns(J, J.run + "_deposit_" + idx + ".q_2d", 0, c, err)) return IMEX_EINVAL;
+    }
+    if (J.topo) {
+      c.assign(1, P(J.B_c, 0));
+      if (!write_columns(J, J.run + "_B_" + idx + ".q_2d", 0, c, err)) return IMEX_EINVAL;
+    }
+  }
+  if (J.phys) {
+    std::vector<const double*> c;
+    for (int i = 0; i < p2d_cols(J.ns); ++i) c.push_back(P(J.p2d, i));
+    if (!write_columns(J, J.run + "_" + idx + ".p_2d", 1, c, err)) return IMEX_EINVAL;
+  }
+  if (J.esri) {
+    const double* h = P(J.esr, 0);
+    const double* T = P(J.esr, 1);
+    if (!write_esri(J, J.run + "_" + idx + ".asc",
+                    [&](size_t c) { return h[c] >= 1.0e-5 ? h[c] : -9999.0; }, err))
+      return IMEX_EINVAL;
+    if (!write_esri(J, J.run + "_T_" + idx + ".asc",
+                    [&](size_t c) { return h[c] >= 1.0e-5 ? T[c] : -9999.0; }, err))
+      return IMEX_EINVAL;
+    auto tot = [&](long off, size_t c) {   // SUM(x(:,j,:),DIM=2)/(1-porosity)
+      double s = 0.0;
+      for (int i = 0; i < J.ns; ++i) s = s + P(off, i)[c];
+      return s / (1.0 - J.porosity);
+    };
+    if (J.settling) {
+      for (int i = 0; i < J.ns; ++i) {
+        const double* d = P(J.dep_e, i);
+        if (!write_esri(J, J.run + "_dep_" + ffmt::lettera(i + 1) + "_" + idx + ".asc",
+                        [&](size_t c) { return d[c] > 0.0 ? d[c] : -9999.0; }, err))
+          return IMEX_EINVAL;
+      }
+      if (!write_esri(J, J.run + "_depTot_" + idx + ".asc",
+                      [&](size_t c) { const double v = tot(J.dep_e, c); return v > 0.0 ? v : -9999.0; },
+                      err))
+        return IMEX_EINVAL;
+    }
+    if (J.erosion) {
+      for (int i = 0; i < J.ns; ++i) {
+        const double* d = P(J.ers_e, i);
+        if (!write_esri(J, J.run + "_ers_" + ffmt::lettera(i + 1) + "_" + idx + ".asc",
+                        [&](size_t c) { return d[c] > 0.0 ? d[c] : -9999.0; }, err))
+          return IMEX_EINVAL;
+      }
+      if (!write_esri(J, J.run + "_ersTot_" + idx + ".asc",
+                      [&](size_t c) { const double v = tot(J.ers_e, c); return v > 0.0 ? v : -9999.0; },
+                      err))
+        return IMEX_EINVAL;
+    }
+  }
+  if (J.maxf) {
+    const double* hm = P(J.hmax, 0);
+    if (!write_esri(J, J.run + "_max.asc",
+                    [&](size_t c) { return hm[c] >= 1.0e-5 ? hm[c] : -9999.0; }, err))
+      return IMEX_EINVAL;
+  }
+  return IMEX_OK;
+}
+
+template <int NS>
+void launch_output_prep(ImexCtx* ctx, const OutputArgs& A) {
+  const long long n = (long long)ctx->P.nx * ctx->P.ny;
+  k_output_prep<NS><<<grid_1d(n, 128), 128, 0, ctx->stream>>>(ctx->P, A);
+  ctx->launches += 1;
+}
+
+void output_prep(ImexCtx* ctx, const OutputArgs& A) {
+  switch (ctx->ns) {
+    case 1: launch_output_prep<1>(ctx, A); break;
+    case 2: launch_output_prep<2>(ctx, A); break;
+    case 3: launch_output_prep<3>(ctx, A); break;
+    default: launch_output_prep<4>(ctx, A); break;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int imex_format_edit(int kind, double value, int w, int d, int e, char* buf, int cap) {
+  if (!buf || cap < 1 || w < 1 || w > 100 || d < 0 || d > 40 || e < 0 || e > 4) return -1;
+  std::string o;
+  switch (kind) {
+    case 0: ffmt::E(o, value, w, d); break;
+    case 1: ffmt::ES(o, value, w, d, e); break;
+    case 2: ffmt::I(o, (long long)value, w); break;
+    case 3: ffmt::F(o, value, w, d); break;
+    default: return -1;
+  }
+  if ((int)o.size() >= cap) return -1;
+  std::memcpy(buf, o.c_str(), o.size() + 1);
+  return (int)o.size();
+}
+
+int imex_gpu_output_wait(ImexCtx* ctx) {
+  if (!ctx) return IMEX_EINVAL;
+  if (ctx->out_thread.joinable()) ctx->out_thread.join();
+  ctx->out_pending = false;
+  const int st = ctx->out_status;
+  ctx->out_status = IMEX_OK;
+  if (st != IMEX_OK) return fail(ctx, st, ctx->out_error);
+  return IMEX_OK;
+}
+
+int imex_gpu_output(ImexCtx* ctx, const ImexOutputSpec* spec) {
+  if (!ctx || !spec || !spec->run_name) return IMEX_EINVAL;
+  int st = imex_gpu_output_wait(ctx);   // one job in flight: the staging buffer is reused
+  if (st != IMEX_OK) return st;
+  CK(cudaSetDevice(ctx->device));
+  const DevParams& P = ctx->P;
+  const ImexParams& hp = ctx->host_params;
+  const int ns = ctx->ns, nv = P.nv;
+  const size_t n = (size_t)P.nx * P.ny;
+  OutJob J;
+  J.run = spec->run_name;
+  J.idx = spec->output_idx;
+  J.nx = P.nx;
+  J.ny = P.ny;
+  J.ns = ns;
+  J.nv = nv;
+  J.threads = spec->threads > 0 ? spec->threads
+                                 : std::max(1, (int)std::thread::hardware_concurrency());
+  J.x0 = P.x0;
+  J.y0 = P.y0;
+  J.dx = P.dx;
+  J.dy = P.dy;
+  J.cell_size = hp.cell_size;
+  J.porosity = hp.erodible_porosity;
+  J.cons = spec->cons != 0;
+  J.phys = spec->phys != 0;
+  J.esri = spec->esri != 0;
+  J.maxf = spec->max_grid != 0;
+  J.erosion = hp.erosion_coeff > 0.0 && ctx->erosion;
+  J.settling = hp.settling_flag && ctx->deposit;
+  J.topo = hp.topo_change_flag && ctx->Bcent;
+  if (J.maxf && !ctx->post_on)
+    return fail(ctx, IMEX_EINVAL, "imex_gpu_output: the _max grid needs imex_gpu_post_init");
+  // staged planes, in order
+  long nplanes = 0;
+  auto take = [&](long k) { const long o = nplanes; nplanes += k; return o; };
+  if (J.cons) {
+    J.q = take(nv);
+    if (J.erosion) { J.ers_c = take(ns); J.erd_c = take(ns); }
+    if (J.settling) J.dep_c = take(ns);
+    if (J.topo) J.B_c = take(1);
+  }
+  if (J.phys) J.p2d = take(p2d_cols(ns));
+  if (J.esri) {
+    J.esr = take(2);
+    if (J.settling) J.dep_e = take(ns);
+    if (J.erosion) J.ers_e = take(ns);
+  }
+  if (J.maxf) J.hmax = take(1);
+  if (nplanes == 0) return IMEX_OK;
+  const size_t dev_need = ((J.phys ? p2d_cols(ns) : 0) + (J.esri ? 2 : 0)) * n;
+  if (dev_need > ctx->out_dev_n) {
+    if (ctx->out_dev) cudaFree(ctx->out_dev);
+    ctx->out_dev = nullptr;
+    ctx->out_dev_n = 0;
+    CK(cudaMalloc((void**)&ctx->out_dev, dev_need * sizeof(double)));
+    ctx->out_dev_n = dev_need;
+  }
+  const size_t host_need = (size_t)nplanes * n;
+  if (host_need > ctx->out_host_n) {
+    if (ctx->out_host) cudaFreeHost(ctx->out_host);
+    ctx->out_host = nullptr;
+    ctx->out_host_n = 0;
+    CK(cudaMallocHost((void**)&ctx->out_host, host_need * sizeof(double)));
+    ctx->out_host_n = host_need;
+  }
+  if (!ctx->out_ev) CK(cudaEventCreateWithFlags(&ctx->out_ev, cudaEventDisableTiming));
+  double* p2d_dev = ctx->out_dev;
+  double* esr_dev = ctx->out_dev + (J.phys ? (size_t)p2d_cols(ns) * n : 0);
+  const size_t row = (size_t)P.nx * sizeof(double), pitch = (size_t)P.pitch * sizeof(double);
+  auto stage_pitched = [&](long off, const double* src, int planes) -> cudaError_t {
+    for (int i = 0; i < planes; ++i) {
+      cudaError_t e = cudaMemcpy2DAsync(ctx->out_host + (size_t)(off + i) * n, row,
+                                        src + (size_t)i * P.plane, pitch, row, P.ny,
+                                        cudaMemcpyDeviceToHost, ctx->stream);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  };
+  OutputArgs A{};
+  A.q = ctx->q;
+  A.deposit = ctx->deposit;
+  A.erosion = ctx->erosion;
+  A.erodible = ctx->erodible;
+  A.Bcent = ctx->Bcent;
+  A.Bx = ctx->Bx;
+  A.By = ctx->By;
+  A.post = ctx->post;
+  A.post_on = ctx->post_on ? 1 : 0;
+  A.p2d = p2d_dev;
+  A.esr = esr_dev;
+  // the order of output_solution: ESRI's qp and the .q_2d zeroing of q, the
+  // .q_2d planes, then the .p_2d values (zeroing DEPOSIT/EROSION), then the
+  // ESRI planes
+  if (J.cons || J.esri) {
+    A.cons = J.cons;
+    A.esri = J.esri;
+    A.phys = 0;
+    output_prep(ctx, A);
+  }
+  if (J.cons) {
+    CK(stage_pitched(J.q, ctx->q, nv));
+    if (J.erosion) {
+      CK(stage_pitched(J.ers_c, ctx->erosion, ns));
+      CK(stage_pitched(J.erd_c, ctx->erodible, ns));
+    }
+    if (J.settling) CK(stage_pitched(J.dep_c, ctx->deposit, ns));
+    if (J.topo) CK(stage_pitched(J.B_c, ctx->Bcent, 1));
+  }
+  if (J.phys) {
+    A.cons = 0;
+    A.esri = 0;
+    A.phys = 1;
+    output_prep(ctx, A);
+    CK(cudaMemcpyAsync(ctx->out_host + (size_t)J.p2d * n, p2d_dev,
+                       (size_t)p2d_cols(ns) * n * sizeof(double), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+  }
+  if (J.esri) {
+    CK(cudaMemcpyAsync(ctx->out_host + (size_t)J.esr * n, esr_dev, 2 * n * sizeof(double),
+                       cudaMemcpyDeviceToHost, ctx->stream));
+    if (J.settling) CK(stage_pitched(J.dep_e, ctx->deposit, ns));
+    if (J.erosion) CK(stage_pitched(J.ers_e, ctx->erosion, ns));
+  }
+  if (J.maxf) CK(stage_pitched(J.hmax, ctx->post.hmax, 1));
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(ctx->out_ev, ctx->stream));
+  J.buf = ctx->out_host;
+  ctx->out_pending = true;
+  ctx->out_status = IMEX_OK;
+  ctx->out_error.clear();
+  cudaEvent_t ev = ctx->out_ev;
+  const int dev = ctx->device;
+  ctx->out_thread = std::thread([ctx, J, ev, dev]() {
+    cudaSetDevice(dev);
+    cudaError_t e = cudaEventSynchronize(ev);
+    if (e != cudaSuccess) {
+      ctx->out_error = std::string("imex_gpu_output: ") + cudaGetErrorString(e);
+      ctx->out_status = IMEX_ECUDA;
+      return;
+    }
+    std::string err;
+    const int st = run_out_job(J, err);
+    if (st != IMEX_OK) {
+      ctx->out_error = "imex_gpu_output: " + err;
+      ctx->out_status = st;
+    }
+  });
   return IMEX_OK;
 }
 

@@ -14,8 +14,8 @@ import os
 
 import numpy as np
 
-from .abi import (IMEX_OK, STATUS_NAMES, ImexParams, ImexPostDiag, ImexStatic,
-                  ImexStats, make_static)
+from .abi import (IMEX_OK, STATUS_NAMES, ImexOutputSpec, ImexParams, ImexPostDiag,
+                  ImexStatic, ImexStats, make_static)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libimexgpu.so")
@@ -74,6 +74,10 @@ def load_library(path=LIB_PATH):
                               + [dp, C.c_int, C.c_int] + [C.c_double] * 3
                               + [dp, C.POINTER(C.c_float)], C.c_int),
         "imex_setup_last_error": ([], C.c_char_p),
+        "imex_gpu_output": ([vp, C.POINTER(ImexOutputSpec)], C.c_int),
+        "imex_gpu_output_wait": ([vp], C.c_int),
+        "imex_format_edit": ([C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_char_p,
+                              C.c_int], C.c_int),
         "imex_gpu_post_init": ([vp, C.c_int, dp, C.c_int, dp], C.c_int),
         "imex_gpu_post_step": ([vp, C.POINTER(ImexPostDiag)], C.c_int),
         "imex_gpu_post_diag": ([vp, C.POINTER(ImexPostDiag)], C.c_int),
@@ -228,6 +232,21 @@ class ImexSolver:
         self._check(self.lib.imex_gpu_post_step(self._h, C.byref(d) if diag else None),
                     "post_step")
         return (d.mass, d.volume, d.area, d.solid_mass) if diag else None
+
+    # -- output_solution (src/inpout_2d.f90:5683-6180) from the device state
+    def output(self, run_name, output_idx, time=0.0, cons=True, phys=True, esri=False,
+               max_grid=False, threads=0):
+        """Write the reference's output files for output number `output_idx`
+        (files carry lettera(output_idx-1)) asynchronously: the call returns
+        once the values are queued on the device; output_wait() waits for the
+        files.  Like the reference, cons sets |q| < 1e-20 to 0 in the state
+        and phys sets DEPOSIT/EROSION below 1e-20 to 0."""
+        spec = ImexOutputSpec(str(run_name).encode(), int(output_idx), float(time), int(cons),
+                              int(phys), int(esri), int(max_grid), int(threads))
+        self._check(self.lib.imex_gpu_output(self._h, C.byref(spec)), "output")
+
+    def output_wait(self):
+        self._check(self.lib.imex_gpu_output_wait(self._h), "output_wait")
 
     def post_diag(self):
         d = ImexPostDiag()
@@ -488,3 +507,14 @@ class ImexMLP:
             self.close()
         except Exception:
             pass
+
+
+def format_edit(kind, value, w, d=0, e=0):
+    """One value through the output writers' Fortran edit descriptors:
+    kind 0 = Ew.d, 1 = ESw.dEe, 2 = Iw, 3 = Fw.d (host code; no GPU)."""
+    L = load_library()
+    buf = C.create_string_buffer(128)
+    n = L.imex_format_edit(int(kind), float(value), int(w), int(d), int(e), buf, 128)
+    if n < 0:
+        raise ValueError("imex_format_edit: bad arguments")
+    return buf.value.decode()

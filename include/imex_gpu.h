@@ -354,6 +354,50 @@ int imex_gpu_ensemble_tuning(ImexEnsemble* ens, int* k_streams, int* n_tried, in
 const char* imex_gpu_ensemble_last_error(ImexEnsemble* ens);
 
 /*
+ * output_solution (src/inpout_2d.f90:5683-6180) from the device state.
+ * imex_gpu_output enqueues, on the context's stream, the values the
+ * reference prints and the copies of them into pinned host memory, then
+ * returns; a host thread formats and writes the files while later steps
+ * run (call imex_gpu_output_wait before reading them; a new
+ * imex_gpu_output waits for the previous one).  Files, named as the
+ * reference names them with idx = lettera(output_idx-1):
+ *   cons:     RUN_idx.q_2d ('(2e20.12,100(e20.12))': x, y, q(1:n_vars)),
+ *             RUN_erosion_idx.q_2d / RUN_erodible_idx.q_2d (erosion_coeff>0),
+ *             RUN_deposit_idx.q_2d (settling_flag), RUN_B_idx.q_2d
+ *             (topo_change_flag); like the reference it sets |q| < 1e-20
+ *             to 0 in the state;
+ *   phys:     RUN_idx.p_2d ('100ES15.7E2') with the columns of :6142-6148
+ *             for this library's physics (no additional gas, liquid,
+ *             stochastic or pore-pressure variables: alphal, shear_vel,
+ *             Rouse_no and inertial_number print as 0, and mu_eff takes the
+ *             excess pore pressure as 0 where the reference reads element 1
+ *             of an empty array); hmax/pdynmax/mod_vel_max come from the
+ *             post-step planes (0 without imex_gpu_post_init); like the
+ *             reference it sets DEPOSIT/EROSION below 1e-20 to 0;
+ *   esri:     RUN_idx.asc (h), RUN_T_idx.asc, RUN_dep_SSSS_idx.asc and
+ *             RUN_depTot_idx.asc (settling_flag), RUN_ers_SSSS_idx.asc and
+ *             RUN_ersTot_idx.asc (erosion_coeff>0), output_esri (:6306-6613);
+ *   max_grid: RUN_max.asc from hmax (output_max, :6195-6235; needs
+ *             imex_gpu_post_init).
+ * The list-directed files of output_esri's first call (dem_esri*.asc) and
+ * the NetCDF output are not written.  threads: formatting threads (0 = all
+ * cores).  A failed write is reported by the next imex_gpu_output_wait.
+ */
+typedef struct ImexOutputSpec {
+  const char* run_name;   /* TRIM(run_name): path prefix of every file */
+  int output_idx;         /* output_idx after the reference's increment */
+  double time;            /* model time of the output (informational) */
+  int cons, phys, esri, max_grid;
+  int threads;
+} ImexOutputSpec;
+int imex_gpu_output(ImexCtx* ctx, const ImexOutputSpec* spec);
+int imex_gpu_output_wait(ImexCtx* ctx);
+/* One value through the writers' Fortran edit descriptors (kind 0 Ew.d,
+ * 1 ESw.dEe, 2 Iw, 3 Fw.d) into buf, NUL-terminated; returns the length, or
+ * -1 for bad arguments.  Host code: needs no GPU. */
+int imex_format_edit(int kind, double value, int w, int d, int e, char* buf, int cap);
+
+/*
  * Set-up on the device (no context needed).  Inputs and outputs are host
  * arrays in the reference's column-major layouts; each call copies its
  * inputs to `device` (< 0: the current one), runs one kernel and copies the

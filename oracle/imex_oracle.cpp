@@ -2745,3 +2745,106 @@ extern "C" int oracle_regrid(int ncols, int nrows, double xll, double yll, doubl
   }
   return status;
 }
+
+// ----------------------------------------------------------- output values
+// The values output_solution prints (src/inpout_2d.f90:5683-6180) and its
+// in-place changes: cons sets |q| < 1e-20 to 0 in q (:5807-5813); phys
+// computes the .p_2d columns from that q (:5914-6148) and sets DEPOSIT and
+// EROSION below 1e-20 to 0 (:6115-6122); esri takes qp(1) and qp(4) of the
+// driver's qp, i.e. of q before the .q_2d zeroing.  p2d: 17+4*ns planes of
+// nx*ny (after x_comp, y_comp): h, u, v, B_out, h+B_out, alphas, T, rho_m,
+// red_grav, DEPOSIT, EROSION, SUM(ERODIBLE)/(1-porosity), alphal, shear_vel,
+// Ri, Rouse_no, mu_eff, hmax, pdynmax, mod_vel_max, inertial_number, for
+// the physics without additional gas, liquid, stochastic or pore-pressure
+// variables (the excess pore pressure of mu_eff is taken as 0).
+extern "C" void oracle_output_prep(OracleCtx* o, int cons, int phys, int esri, double* p2d,
+                                   double* esr) {
+  const int nx = o->nx, ny = o->ny, nv = o->nv, ns = o->ns, np = o->np;
+  const size_t N = (size_t)nx * ny;
+  const ImexParams& p = o->p;
+  auto t0 = [](double v) { return (std::fabs(v) < 1.0e-20) ? 0.0 : v; };
+  for (int k = 1; k <= ny; ++k) {
+    for (int j = 1; j <= nx; ++j) {
+      const size_t c = o->c2(j, k);
+      double* q = &o->q[(size_t)nv * c];
+      double qp[MAXV], p_dyn = 0.0;
+      if (esri) {
+        o->qc_to_qp(q, qp, p_dyn);
+        esr[c] = qp[0];
+        esr[N + c] = qp[3];
+      }
+      if (cons)
+        for (int i = 0; i < nv; ++i)
+          if (std::fabs(q[i]) < 1.0e-20) q[i] = 0.0;
+      if (!phys) continue;
+      o->qc_to_qp(q, qp, p_dyn);
+      double r_Ri, r_rho_m, r_rho_c, r_red_grav, spc, spm;
+      o->mixt_var(qp, r_Ri, r_rho_m, r_rho_c, r_red_grav, false, spc, spm);
+      double r_h = qp[0], r_u = qp[nv], r_v = qp[nv + 1], r_T = qp[3];
+      double al[MAXS], mu_eff = 0.0, inertial = 0.0, r_alphal = 0.0;
+      const double shear_vel = 0.0;
+      if (r_h > 0.0) {
+        for (int i = 0; i < ns; ++i) al[i] = p.alpha_flag ? qp[4 + i] : qp[4 + i] / r_h;
+        if (p.rheology_flag && p.rheology_model == 1) {
+          const double dp = fmax_f(0.0, 0.0);
+          mu_eff = p.mu * fmax_f(0.0, 1.0 - dp / (r_rho_m * r_h * r_red_grav));
+        }
+      } else {
+        for (int i = 0; i < ns; ++i) al[i] = 0.0;
+      }
+      r_h = t0(r_h);
+      r_u = t0(r_u);
+      r_v = t0(r_v);
+      const double B = o->B_cent.empty() ? 0.0 : o->B_cent[c];
+      const double B_out = t0(B);
+      double dep[MAXS], ers[MAXS];
+      for (int i = 0; i < ns; ++i) {
+        al[i] = t0(al[i]);
+        dep[i] = o->deposit.empty() ? 0.0 : o->deposit[c + N * i];
+        ers[i] = o->erosion.empty() ? 0.0 : o->erosion[c + N * i];
+        if (std::fabs(dep[i]) < 1.0e-20) {
+          dep[i] = 0.0;
+          if (!o->deposit.empty()) o->deposit[c + N * i] = 0.0;
+        }
+        if (std::fabs(ers[i]) < 1.0e-20) {
+          ers[i] = 0.0;
+          if (!o->erosion.empty()) o->erosion[c + N * i] = 0.0;
+        }
+      }
+      r_T = t0(r_T);
+      r_rho_m = t0(r_rho_m);
+      r_red_grav = t0(r_red_grav);
+      r_alphal = t0(r_alphal);
+      mu_eff = t0(mu_eff);
+      inertial = t0(inertial);
+      double esum = 0.0;
+      for (int i = 0; i < ns; ++i)
+        esum = esum + (o->erodible.empty() ? 0.0 : o->erodible[(size_t)i + ns * c]);
+      const double etot = esum / (1.0 - p.erodible_porosity);
+      int col = 0;
+      auto put = [&](double v) { p2d[(size_t)col++ * N + c] = v; };
+      put(r_h);
+      put(r_u);
+      put(r_v);
+      put(B_out);
+      put(r_h + B_out);
+      for (int i = 0; i < ns; ++i) put(al[i]);
+      put(r_T);
+      put(r_rho_m);
+      put(r_red_grav);
+      for (int i = 0; i < ns; ++i) put(dep[i]);
+      for (int i = 0; i < ns; ++i) put(ers[i]);
+      put(etot);
+      put(r_alphal);
+      put(shear_vel);
+      put(r_Ri);
+      for (int i = 0; i < ns; ++i) put(0.0);
+      put(mu_eff);
+      put(o->hmax.empty() ? 0.0 : o->hmax[c]);
+      put(o->pdynmax.empty() ? 0.0 : o->pdynmax[c]);
+      put(o->mvmax.empty() ? 0.0 : o->mvmax[c]);
+      put(inertial);
+      (void)np;
+    }
+  }
+}

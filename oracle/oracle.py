@@ -78,6 +78,7 @@ def lib():
         L.oracle_regrid.restype = C.c_int
         L.oracle_regrid.argtypes = ([C.c_int, C.c_int] + [C.c_double] * 4 + [dp, C.c_int, C.c_int]
                                     + [C.c_double] * 3 + [dp])
+        L.oracle_output_prep.argtypes = [vp, C.c_int, C.c_int, C.c_int, dp, dp]
         L.oracle_limit.restype = C.c_double
         L.oracle_limit.argtypes = [C.c_double] * 6 + [C.c_int, C.c_double]
         _LIB = L
@@ -182,6 +183,16 @@ class Oracle:
         t = np.ascontiguousarray(t, dtype=np.float64)
         d = np.ascontiguousarray(d, dtype=np.float64)
         lib().oracle_post_init(self._h, len(t), _p(t), len(d), _p(d))
+
+    def output_prep(self, cons, phys, esri):
+        """(p2d (17+4ns, nx, ny), esr (2, nx, ny)) of output_solution, with its
+        in-place changes to q, DEPOSIT and EROSION."""
+        nx, ny, ns = self.nx, self.ny, self.ns
+        p2d = np.zeros((17 + 4 * ns) * nx * ny)
+        esr = np.zeros(2 * nx * ny)
+        lib().oracle_output_prep(self._h, int(cons), int(phys), int(esri), _p(p2d), _p(esr))
+        return (p2d.reshape(17 + 4 * ns, ny, nx).transpose(0, 2, 1),
+                esr.reshape(2, ny, nx).transpose(0, 2, 1))
 
     def post_diag(self):
         out = np.zeros(4)
