@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-setup", action="store_true")
+    ap.add_argument("--output-n", type=int, default=1024,
+                    help="grid side of the output measurement (0 = skip)")
     ap.add_argument("--learned-pairs", type=int, default=10_000_000)
     ap.add_argument("--learned-n", type=int, default=1024, help="side of the comparison grid")
     return ap.parse_args()
@@ -282,6 +284,39 @@ def run_setup(args):
     return out
 
 
+def run_output(args, g, p, steps):
+    """output_solution from the device at the benchmark's size: the
+    .q_2d/.p_2d/ESRI files of one output written by the library's host
+    thread while `steps` further steps run, against the same steps without
+    output (the cost the output adds to the run)."""
+    import tempfile
+    import torch
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        run = os.path.join(d, "bench")
+        g.sync()
+        t0 = time.perf_counter()
+        g.advance(steps)
+        g.sync()
+        base = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        g.output(run, 1, cons=True, phys=True, esri=True)
+        t_enq = time.perf_counter() - t0
+        g.advance(steps)
+        g.sync()
+        t_steps = time.perf_counter() - t0
+        g.output_wait()
+        t_all = time.perf_counter() - t0
+        size = sum(os.path.getsize(os.path.join(d, f)) for f in os.listdir(d))
+        nfiles = len(os.listdir(d))
+    out = {"files": nfiles, "bytes": size, "enqueue_ms": t_enq * 1e3,
+           "steps_after_output": steps, "steps_ms_without_output": base * 1e3,
+           "steps_ms_with_output": t_steps * 1e3, "output_done_ms": t_all * 1e3,
+           "text_MB_per_s": size / 1e6 / t_all, "threads": os.cpu_count(),
+           "timing": "host clock; the files are formatted while the steps run"}
+    return out
+
+
 def run_learned(args, g, p):
     """Learned vs plain Newton start (fifth workload): pairs harvested from the
     benchmark's own 4096^2 fractal run (third workload), the network trained
@@ -495,6 +530,16 @@ def main():
     setup = None
     if rank == 0 and world == 1 and not args.no_setup:
         setup = run_setup(args)
+    output = None
+    if rank == 0 and world == 1 and args.output_n > 0:
+        po, sto, qo = workload(args.output_n, args.layer)
+        go = ImexSolver(po, sto, device=local)
+        go.set_state(qo, 0.0)
+        go.set_clock(0.0, 1e-2)
+        go.advance(3)
+        output = run_output(args, go, po, 20)
+        output["grid"] = [args.output_n, args.output_n]
+        go.close()
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(args)
@@ -527,6 +572,7 @@ def main():
             "ensemble": ensemble,
             "learned_vs_plain": learned,
             "setup": setup,
+            "output": output,
         }
         print(json.dumps(line), flush=True)
     g.close()

@@ -49,6 +49,8 @@ int main(void) {
   printf("ImexParams %zu\nImexStatic %zu\nImexStats %zu\nImexBC %zu\nImexPostDiag %zu\n",
          sizeof(ImexParams), sizeof(ImexStatic), sizeof(ImexStats), sizeof(ImexBC),
          sizeof(ImexPostDiag));
+  printf("ImexOutputSpec %zu\n", sizeof(ImexOutputSpec));
+  OFF(ImexOutputSpec, time); OFF(ImexOutputSpec, cons); OFF(ImexOutputSpec, threads);
   OFF(ImexParams, limiter); OFF(ImexParams, cfl); OFF(ImexParams, bcW); OFF(ImexParams, bcN);
   OFF(ImexParams, grav); OFF(ImexParams, rho_s); OFF(ImexParams, time_param);
   OFF(ImexParams, erodible_fract); OFF(ImexParams, coeff_porosity);
@@ -76,6 +78,7 @@ def test_ctypes_mirror_matches_c_layout():
     assert c["ImexStats"] == C.sizeof(abi.ImexStats)
     assert c["ImexBC"] == C.sizeof(abi.ImexBC)
     assert c["ImexPostDiag"] == C.sizeof(abi.ImexPostDiag)
+    assert c["ImexOutputSpec"] == C.sizeof(abi.ImexOutputSpec)
     for key, v in c.items():
         if "." in key:
             t, f = key.split(".")
