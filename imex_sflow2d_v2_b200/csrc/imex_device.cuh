@@ -31,6 +31,22 @@
 #ifndef IMEX_NOINL
 #define IMEX_NOINL __device__ __noinline__
 #endif
+// Per function, measured on the 4096^2 workload: x**y and the settling
+// velocity stay out of line (inlined, erosion 9.3 -> 10.7 ms); the
+// conserved <-> physical conversions and the limiter are inlined (flux
+// 11.1 -> 10.2 ms, first Newton pass 6.1 -> 5.6, erosion 9.3 -> 8.8).
+#ifndef IMEX_IPOW_FN
+#define IMEX_IPOW_FN IMEX_NOINL
+#endif
+#ifndef IMEX_QCQP_FN
+#define IMEX_QCQP_FN __device__ __forceinline__
+#endif
+#ifndef IMEX_LIMIT_FN
+#define IMEX_LIMIT_FN __device__ __forceinline__
+#endif
+#ifndef IMEX_SETTLE_FN
+#define IMEX_SETTLE_FN IMEX_NOINL
+#endif
 // Functions with one or two call sites per kernel (the Newton pieces, the
 // mass-exchange terms) are inlined: their per-cell arrays then live in
 // registers instead of being passed through the stack.
@@ -133,7 +149,7 @@ IMEX_HD void two_prod(double a, double b, double& p, double& e) {
   p = a * b;
   e = fma(a, b, -p);
 }
-IMEX_NOINL double ipow(double x, double y) {
+IMEX_IPOW_FN double ipow(double x, double y) {
   if (isnan(x) || isnan(y)) return x + y;
   if (x == 0.0 && y != 0.0) return (y > 0.0) ? 0.0 : __longlong_as_double(0x7ff0000000000000LL);
   if (x < 0.0 && y != 0.0) return __longlong_as_double(0x7ff8000000000000LL);
@@ -297,7 +313,7 @@ IMEX_HD double sp_heat_c_of(const DevParams& P, const double* qpj, double rho_m)
 // ----------------------------------------------------------- qc_to_qp
 // r_phys_var + qc_to_qp; also returns red_grav through the out pointer.
 template <int NS>
-IMEX_NOINL void qc_to_qp(const DevParams& P, const double* qc, double* qp,
+IMEX_QCQP_FN void qc_to_qp(const DevParams& P, const double* qc, double* qp,
                          double* p_dyn = nullptr) {
   constexpr int NV = 4 + NS;
   if (!(qc[0] > EPS)) {
@@ -394,7 +410,7 @@ IMEX_HD void cell_qp(const DevParams& P, const double* qc, double* qp) {
 
 // ----------------------------------------------------------- qp_to_qc
 template <int NS>
-IMEX_NOINL void qp_to_qc(const DevParams& P, const double* qp, double* qc) {
+IMEX_QCQP_FN void qp_to_qc(const DevParams& P, const double* qp, double* qc) {
   constexpr int NV = 4 + NS;
   double r_h = qp[0];
   if (!(r_h > EPS)) {
@@ -450,7 +466,7 @@ IMEX_HD double maxmod(double a, double b) {
   double sa = a / fabs(a), sb = b / fabs(b);
   return 0.5 * (sa + sb) * fmax_f(fabs(a), fabs(b));
 }
-IMEX_NOINL double limit(double v1, double v2, double v3, double z1, double z2, double z3,
+IMEX_LIMIT_FN double limit(double v1, double v2, double v3, double z1, double z2, double z3,
                         int lim, double theta) {
   if (lim == 1) {
     // minmod(a,b) with a=(v3-v2)/(z3-z2), b=(v2-v1)/(z2-z1), z increasing:
@@ -830,7 +846,7 @@ IMEX_HD void semi_impl_terms(const DevParams& P, double bx, double by, double bx
 }
 
 // ------------------------------------------------------ mass exchange
-IMEX_NOINL double settling_velocity(const DevParams& P, double diam, double rhos, double rhoc,
+IMEX_SETTLE_FN double settling_velocity(const DevParams& P, double diam, double rhos, double rhoc,
                                  double ikv) {
   double inv_sqrt_C_D = 1.0;
   if (rhos <= rhoc) return 0.0;

@@ -2,7 +2,7 @@
 // (src/inpout_2d.f90: '(2e20.12,100(e20.12))' for .q_2d, '100ES15.7E2' for
 // .p_2d, '(2000ES12.3E3)', '(A,I5)', '(A,F15.3)' for the ESRI grids), as
 // gfortran writes them: the decimal digits are the correctly rounded ones
-// (the C library's %e/%f conversions), Ew.d writes 0.d1...dd with a two-
+// (std::to_chars for %e-style digits, %f for Fw.d), Ew.d writes 0.d1...dd with a two-
 // digit exponent after 'E' (three digits and no 'E' from 100 to 999),
 // ESw.dEe writes d1.d2...E with exactly e exponent digits, a value whose
 // exponent does not fit and any field too narrow become w asterisks, a
@@ -10,6 +10,7 @@
 // written as NaN / Infinity right-justified.  Host code only.
 #pragma once
 
+#include <charconv>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -48,13 +49,15 @@ inline bool special(std::string& out, double v, int w) {
 // correctly rounded: |v| = 0.D1D2..Dsig x 10^E10 (E10 for the 0.d form).
 inline void digits(double a, int sig, char* dig, int& e10) {
   char buf[64];
-  std::snprintf(buf, sizeof buf, "%.*e", sig - 1, a);   // d.ddde+XX
+  const auto r = std::to_chars(buf, buf + sizeof buf - 1, a, std::chars_format::scientific,
+                               sig - 1);   // d.ddde+XX, correctly rounded
+  *r.ptr = 0;
   int k = 0;
-  for (const char* p = buf; *p && *p != 'e'; ++p)
+  const char* p = buf;
+  for (; *p && *p != 'e'; ++p)
     if (*p >= '0' && *p <= '9') dig[k++] = *p;
   dig[k] = 0;
-  const char* ep = std::strchr(buf, 'e');
-  e10 = std::atoi(ep + 1);
+  e10 = std::atoi(p + 1);
 }
 
 // Ew.d

@@ -2278,13 +2278,28 @@ bool write_esri(const OutJob& J, const std::string& path, F val, std::string& er
   ffmt::I(o, -9999, 5);
   o += "\n";
   bool ok = std::fwrite(o.data(), 1, o.size(), f) == o.size();
-  for (int k = J.ny; k >= 1 && ok; --k) {
-    o.clear();
-    for (int j = 1; j <= J.nx; ++j) {
-      ffmt::ES(o, val((size_t)(j - 1) + (size_t)(k - 1) * J.nx), 12, 3, 3);
-      if (j % 2000 == 0 || j == J.nx) o.push_back('\n');
+  // rows from north to south, formatted in bands by J.threads workers
+  const int T = std::max(1, J.threads), band = 16;
+  std::vector<std::string> text(T);
+  for (int r0 = 0; r0 < J.ny && ok; r0 += band * T) {
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; ++t) {
+      th.emplace_back([&, t]() {
+        std::string& b = text[t];
+        b.clear();
+        const int ra = r0 + t * band, rb = std::min(J.ny, ra + band);
+        for (int r = ra; r < rb; ++r) {
+          const int k = J.ny - r;
+          for (int j = 1; j <= J.nx; ++j) {
+            ffmt::ES(b, val((size_t)(j - 1) + (size_t)(k - 1) * J.nx), 12, 3, 3);
+            if (j % 2000 == 0 || j == J.nx) b.push_back('\n');
+          }
+        }
+      });
     }
-    ok = std::fwrite(o.data(), 1, o.size(), f) == o.size();
+    for (auto& x : th) x.join();
+    for (int t = 0; t < T && ok; ++t)
+      if (!text[t].empty()) ok = std::fwrite(text[t].data(), 1, text[t].size(), f) == text[t].size();
   }
   if (std::fclose(f) != 0) ok = false;
   if (!ok) err = "write failed: " + path;
