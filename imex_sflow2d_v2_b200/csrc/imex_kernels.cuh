@@ -896,6 +896,9 @@ IMEX_FLAT bool newton_iterk(const DevParams& P, double* qj, const double* qj_old
     mx = (i == 0) ? r : fmax_f(mx, r);
   }
   double alamin = EPS / mx;
+  bool xfin = true;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) xfin &= isfinite(x_old[i]);
   if (alamin == 0.0) {
 #pragma unroll
     for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i];
@@ -908,9 +911,32 @@ IMEX_FLAT bool newton_iterk(const DevParams& P, double* qj, const double* qj_old
       for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i] + alam * dd[i];
 #pragma unroll
       for (int i = 0; i < NV; ++i) qt[i] = qj_rel[i] * qj_org[i];
-      eval_f<NS>(P, qt, qj_old, Rj, bx, by, dt, rt, scal_f);
+      // Rows other than 2, 3 carry no implicit term: eval_f's sum of f^2
+      // taken over them alone, in eval_f's order, cannot exceed the full
+      // sum (rounded addition of a term >= 0 never decreases a sum, and
+      // rounding is monotone).  When that partial half-sum already exceeds
+      // 0.9*scal_f_old the trial fails whatever the implicit terms are, and
+      // the implicit terms are not evaluated.  Only for trials whose failure
+      // is all that matters: not trial 0 and not alam = 1 (their scal_f
+      // sets the next alam), and with a finite old iterate (then the
+      // residual left by the last trial is never read: a search that puts
+      // the old iterate back ends the iteration as converged).
+      bool fails = false;
+      if (trial > 0 && alam != 1.0 && xfin) {
+        double d = 0.0;
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+          if (i == 1 || i == 2) continue;
+          const double R = Rj[i] - 1.0 * 0.0;
+          const double fi = qt[i] - qj_old[i] + dt * R;
+          const double f = 1.0 * fi;
+          d += f * f;
+        }
+        fails = 0.5 * d > 0.9 * scal_f_old;
+      }
+      if (!fails) eval_f<NS>(P, qt, qj_old, Rj, bx, by, dt, rt, scal_f);
       ++trials;
-      if (scal_f <= 0.9 * scal_f_old) break;
+      if (!fails && scal_f <= 0.9 * scal_f_old) break;
       if (alam < alamin) {
 #pragma unroll
         for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i];
