@@ -1011,12 +1011,14 @@ IMEX_FLAT void mass_exchange(const DevParams& P, const double* qpj, double bx, d
   Mixt m = mixt_var<NS>(P, qpj);
   double spc = sp_heat_c_of<NS>(P, qpj, m.rho_m);
   double ikv = 1.0 / P.kin_visc_c;
+  double hind = -1.0;   // the hindered-settling factor, the same for every class
 #pragma unroll
   for (int i = 0; i < NS; ++i) {
     if (al[i] > 0.0 && P.settling_flag) {
       double sv = settling_velocity(P, P.diam_s[i], P.rho_s[i], m.rho_c, ikv);
       dep[i] = al[i] * sv * 1.0;
-      dep[i] = dep[i] * ipow(1.0 - fmin_f(1.0, at / alpha_max), hind_exp);
+      if (hind < 0.0) hind = ipow(1.0 - fmin_f(1.0, at / alpha_max), hind_exp);
+      dep[i] = dep[i] * hind;
       dep[i] = fmin_f(dep[i], r_h * al[i] / dtl);
       if (dep[i] < 0.0) dep_neg = true;
     }
