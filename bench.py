@@ -65,6 +65,11 @@ def parse():
     return ap.parse_args()
 
 
+def workload_name(n):
+    return ("fractal-dem inlet %dx%d, 10 m cells, 3 solid classes, settling+erosion, Voellmy, "
+            "2 m initial layer" % (n, n))
+
+
 def workload(n, layer):
     from imex_sflow2d_v2_b200 import configs
     return configs.fractal_inlet(n=n, initial_layer=layer)
@@ -388,9 +393,10 @@ def run_reference(args, rank, world):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "fractal-dem inlet, 3 solid classes, settling+erosion "
-                                   "(CPU sample %dx%d)" % (args.cpu_n, args.cpu_n),
-                       "grid": [args.cpu_n, args.cpu_n], "parallelism": "openmp"},
+            "config": {"workload": workload_name(args.n), "grid": [args.n, args.n],
+                       "cells": args.n * args.n, "parallelism": "host threads (OpenMP)",
+                       "sample": "each step times a %dx%d instance of the same generator "
+                                 "(cpu_baseline.sample)" % (args.cpu_n, args.cpu_n)},
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
@@ -549,8 +555,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "fractal-dem inlet %dx%d, 10 m cells, 3 solid classes, "
-                                   "settling+erosion, Voellmy, 2 m initial layer" % (n, n),
+            "config": {"workload": workload_name(n),
                        "grid": [n, n], "cells": cells, "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs larger than L2 (state %.2f GB)" % (8 * (4 + p.n_solid) * cells / 1e9),
                        "solve_cells_per_step": int(s1.solve_cells)},
