@@ -176,6 +176,9 @@ cudaError_t launch_flux_ns(ImexCtx* ctx) {
   if (!attr_set) {
     cudaError_t e = cudaFuncSetAttribute(k_flux<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_flux<NS>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
     attr_set = true;
   }
   k_flux<NS><<<tile_grid(P), FLUX_THREADS, smem, ctx->stream>>>(
@@ -1779,7 +1782,7 @@ __global__ void __launch_bounds__(FLUX_THREADS)
   constexpr int NV = 4 + NS, NP = 6 + NS;
   const DevParams& P = Pp;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  FluxShared<NS>& S = *reinterpret_cast<FluxShared<NS>*>(smem_raw);
+  CflShared<NS>& S = *reinterpret_cast<CflShared<NS>*>(smem_raw);
   const int j0 = blockIdx.x * TX, k0 = blockIdx.y * TY;
   const int nx = P.nx, ny = P.ny;
   const long long tile = (long long)blockIdx.y * gridDim.x + blockIdx.x;
@@ -1898,7 +1901,7 @@ __global__ void __launch_bounds__(1024) k_cfl_fold(const __grid_constant__ DevPa
 template <int NS>
 cudaError_t launch_cfl_tiles(ImexCtx* ctx, double* scratch) {
   const DevParams& P = ctx->P;
-  size_t smem = sizeof(FluxShared<NS>);
+  size_t smem = sizeof(CflShared<NS>);
   cudaError_t e = cudaFuncSetAttribute(k_cfl_tiles<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
