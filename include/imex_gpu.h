@@ -380,7 +380,7 @@ const char* imex_gpu_ensemble_last_error(ImexEnsemble* ens);
  *   max_grid: RUN_max.asc from hmax (output_max, :6195-6235; needs
  *             imex_gpu_post_init).
  * The list-directed files of output_esri's first call (dem_esri*.asc) and
- * the NetCDF output are not written.  threads: formatting threads (0 = all
+ * the NetCDF-4 output are not written.  threads: formatting threads (0 = all
  * cores).  A failed write is reported by the next imex_gpu_output_wait.
  */
 typedef struct ImexOutputSpec {
