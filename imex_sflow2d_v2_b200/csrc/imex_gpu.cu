@@ -111,6 +111,18 @@ cudaError_t dalloc(T** p, size_t n) {
 
 int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
 
+// Function attributes belong to a device: `mask` records, per device
+// index, that the attribute has been set there.
+bool attr_needed(unsigned long long& mask) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return true;
+  return (mask & (1ULL << dev)) == 0;
+}
+void attr_done(unsigned long long& mask) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64) mask |= 1ULL << dev;
+}
+
 // Upload an (nx,ny) Fortran plane into a pitched device plane.
 cudaError_t upload_plane(ImexCtx* ctx, double* dst, const double* src, double fill) {
   const int nx = ctx->P.nx, ny = ctx->P.ny;
@@ -172,14 +184,14 @@ template <int NS>
 cudaError_t launch_flux_ns(ImexCtx* ctx) {
   const DevParams& P = ctx->P;
   size_t smem = sizeof(FluxShared<NS>);
-  static bool attr_set = false;
-  if (!attr_set) {
+  static unsigned long long attr_set = 0;
+  if (attr_needed(attr_set)) {
     cudaError_t e = cudaFuncSetAttribute(k_flux<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_flux<NS>, cudaFuncAttributePreferredSharedMemoryCarveout,
                              (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
-    attr_set = true;
+    attr_done(attr_set);
   }
   k_flux<NS><<<tile_grid(P), FLUX_THREADS, smem, ctx->stream>>>(
       ctx->P, ctx->q, ctx->mask, ctx->cellinfo, ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy, ctx->Byy,
@@ -1203,11 +1215,11 @@ int mlp_refresh_bf16(ImexMLP* mlp) {
 }
 
 int mlp_grad_pass(ImexMLP* mlp, const float* x, const float* y, long long n) {
-  static bool attr = false;
-  if (!attr) {
+  static unsigned long long attr = 0;
+  if (attr_needed(attr)) {
     CKM(cudaFuncSetAttribute(mlp::k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)mlp::SMEM_GRAD));
-    attr = true;
+    attr_done(attr);
   }
   const long long tiles = (n + mlp::SAMPLES - 1) / mlp::SAMPLES;
   const int grid = (int)std::max<long long>(1, std::min<long long>(tiles, 148));
@@ -1398,13 +1410,13 @@ const char* imex_mlp_last_error(ImexMLP* mlp) { return mlp ? mlp->last_error.c_s
 namespace {
 template <int NS>
 cudaError_t launch_warm_predict_ns(ImexCtx* ctx) {
-  static bool attr = false;
-  if (!attr) {
+  static unsigned long long attr = 0;
+  if (attr_needed(attr)) {
     cudaError_t e = cudaFuncSetAttribute(k_warm_predict<NS>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)mlp::SMEM_NET);
     if (e != cudaSuccess) return e;
-    attr = true;
+    attr_done(attr);
   }
   WarmNorm nrm;
   const float* n = ctx->warm_mlp->norm;
