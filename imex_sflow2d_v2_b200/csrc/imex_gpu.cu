@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -112,15 +113,18 @@ cudaError_t dalloc(T** p, size_t n) {
 int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
 
 // Function attributes belong to a device: `mask` records, per device
-// index, that the attribute has been set there.
-bool attr_needed(unsigned long long& mask) {
+// index, that the attribute has been set there.  Host threads may race to
+// set the same attribute; setting it twice is harmless, and the mask is an
+// atomic so that the record itself is well defined.
+bool attr_needed(std::atomic<unsigned long long>& mask) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return true;
-  return (mask & (1ULL << dev)) == 0;
+  return (mask.load(std::memory_order_acquire) & (1ULL << dev)) == 0;
 }
-void attr_done(unsigned long long& mask) {
+void attr_done(std::atomic<unsigned long long>& mask) {
   int dev = 0;
-  if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64) mask |= 1ULL << dev;
+  if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64)
+    mask.fetch_or(1ULL << dev, std::memory_order_acq_rel);
 }
 
 // Upload an (nx,ny) Fortran plane into a pitched device plane.
@@ -184,7 +188,7 @@ template <int NS>
 cudaError_t launch_flux_ns(ImexCtx* ctx) {
   const DevParams& P = ctx->P;
   size_t smem = sizeof(FluxShared<NS>);
-  static unsigned long long attr_set = 0;
+  static std::atomic<unsigned long long> attr_set{0};
   if (attr_needed(attr_set)) {
     cudaError_t e = cudaFuncSetAttribute(k_flux<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -1215,7 +1219,7 @@ int mlp_refresh_bf16(ImexMLP* mlp) {
 }
 
 int mlp_grad_pass(ImexMLP* mlp, const float* x, const float* y, long long n) {
-  static unsigned long long attr = 0;
+  static std::atomic<unsigned long long> attr{0};
   if (attr_needed(attr)) {
     CKM(cudaFuncSetAttribute(mlp::k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)mlp::SMEM_GRAD));
@@ -1410,7 +1414,7 @@ const char* imex_mlp_last_error(ImexMLP* mlp) { return mlp ? mlp->last_error.c_s
 namespace {
 template <int NS>
 cudaError_t launch_warm_predict_ns(ImexCtx* ctx) {
-  static unsigned long long attr = 0;
+  static std::atomic<unsigned long long> attr{0};
   if (attr_needed(attr)) {
     cudaError_t e = cudaFuncSetAttribute(k_warm_predict<NS>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1778,8 +1782,10 @@ static __device__ __align__(256) double g_noalloc_dt[NOALLOC_MAX_TILES + 1];
 namespace {
 // Device address of g_noalloc_dt, looked up once per device (host code may
 // not use the symbol's name as a device address).
+// Atomic, so that two host threads making their first call on one device
+// at once both store the same address without a data race.
 constexpr int NOALLOC_MAX_DEVICES = 64;
-double* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
+std::atomic<double*> g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
 
 // Per-tile CFL minimum.  k_flux takes its speeds from the stage view and,
 // when an inlet-interior cell is in the stencil, from the timestep view;
@@ -1937,13 +1943,14 @@ extern "C" int imex_gpu_timestep_noalloc(ImexCtx* ctx, double* dt) {
                     std::to_string(NOALLOC_MAX_TILES));
   if (ctx->device < 0 || ctx->device >= NOALLOC_MAX_DEVICES)
     return fail(ctx, IMEX_EINVAL, "imex_gpu_timestep_noalloc: device index out of range");
-  if (!g_noalloc_ptr[ctx->device]) {
+  double* scratch = g_noalloc_ptr[ctx->device].load(std::memory_order_acquire);
+  if (!scratch) {
     // first call on this device: resolve the scratch array's device address
     void* ptr = nullptr;
     CK(cudaGetSymbolAddress(&ptr, g_noalloc_dt));
-    g_noalloc_ptr[ctx->device] = static_cast<double*>(ptr);
+    scratch = static_cast<double*>(ptr);
+    g_noalloc_ptr[ctx->device].store(scratch, std::memory_order_release);
   }
-  double* scratch = g_noalloc_ptr[ctx->device];
   if (ctx->P.cfl == -1.0) {
     *dt = ctx->P.max_dt;
     return IMEX_OK;

@@ -196,10 +196,12 @@ int imex_gpu_timestep(ImexCtx* ctx, double* dt);
  * 1,048,576 tiles (about 268 million cells) are rejected with IMEX_EINVAL
  * and a message in imex_gpu_last_error.  Inputs are the context's state and
  * mask (from imex_gpu_check_solve); the output is *dt on the host.  Unlike
- * imex_gpu_timestep it leaves the stage-1 fluxes uncomputed.  The first call
- * on a device looks up the array's device address; make that first call
- * before any stream capture.  All calls share the array: calls that overlap
- * on one GPU race with each other. */
+ * imex_gpu_timestep it leaves the stage-1 fluxes uncomputed.  The call is
+ * synchronous: it copies dt to the caller's host variable and waits for its
+ * stream, so it must not be called while its stream (or, in global capture
+ * mode, any stream) is being captured into a CUDA graph.  The first call on
+ * a device also looks up the array's device address.  All calls share the
+ * array: calls that overlap on one GPU race with each other. */
 int imex_gpu_timestep_noalloc(ImexCtx* ctx, double* dt);
 int imex_gpu_rk_step(ImexCtx* ctx, double t, double dt);
 int imex_gpu_erosion_deposition(ImexCtx* ctx, double dt);

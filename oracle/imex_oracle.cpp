@@ -231,6 +231,13 @@ struct OracleCtx {
   std::vector<int32_t> epL, epR, epB, epT;  // reconstruction epoch of the last write
   int32_t recon_epoch = 0;
   std::atomic<int64_t> stale_wet_reads{0};
+  // mass budget (test instrument): cumulative changes of SUM(q(1,:,:)) by
+  // cause since set_state, in units of q(1) (multiply by dx*dy for mass):
+  // [0] fluxes through faces with exactly one solved side (domain border,
+  // inlet ring), from the face fluxes alone; [1] assembly fixes; [2] the
+  // erosion/deposition update; [3] term [0] of the last step only
+  long double mass_budget[4] = {0.0L, 0.0L, 0.0L, 0.0L};
+  long double stage_face_flux[4] = {0.0L, 0.0L, 0.0L, 0.0L};
 
   double t = 0.0, dt = 0.0, dt_old = 0.0, dt_old_old = 0.0, t_end = 1e300,
          t_output = -1.0;
@@ -255,13 +262,18 @@ struct OracleCtx {
   inline double* FX(std::vector<double>& a, int n, int j, int k) { return &a[(size_t)n * sx2(j, k)]; }
   inline double* FY(std::vector<double>& a, int n, int j, int k) { return &a[(size_t)n * sy2(j, k)]; }
 
+  // may be called from parallel loops: the result (OR of codes, lowest
+  // cell index and code) does not depend on the order of the calls
   void record_error(int code, int j, int k) {
-    error_mask |= IMEX_ERRBIT(code);
     int64_t idx = (int64_t)c2(j, k);
-    if (first_err_index < 0 || idx < first_err_index ||
-        (idx == first_err_index && code < first_err_code)) {
-      first_err_index = idx;
-      first_err_code = code;
+#pragma omp critical(oracle_record_error)
+    {
+      error_mask |= IMEX_ERRBIT(code);
+      if (first_err_index < 0 || idx < first_err_index ||
+          (idx == first_err_index && code < first_err_code)) {
+        first_err_index = idx;
+        first_err_code = code;
+      }
     }
   }
 
@@ -1022,7 +1034,9 @@ void OracleCtx::reconstruction(const double* q_expl, const double* qp_expl,
     double qrec_stencil[3] = {0, 0, 0}, x_stencil[3] = {0, 0, 0}, y_stencil[3] = {0, 0, 0};
     auto QPC = [&](int jj, int kk) -> const double* { return qp_expl + (size_t)np * c2(jj, kk); };
     auto QPE = [&](int i, int jj, int kk) -> double {
+#ifndef ORACLE_TIMING
       if (stage_arrays && !mask[c2(jj, kk)]) note_stage_read(jj, kk);
+#endif
       return QPC(jj, kk)[i - 1];
     };
     const size_t cc = c2(j, k);
@@ -1343,8 +1357,12 @@ void OracleCtx::eval_speeds() {
     for (int64_t l = 0; l < solve_interfaces_x; ++l) {
       int j = j_stag_x[l], k = k_stag_x[l];
       size_t f = sx2(j, k);
+#ifndef ORACLE_TIMING
       if (epL[f] != recon_epoch && face_wet(FX(qpL, np, j, k), idx_u)) ++stale_wet_reads;
+#endif
+#ifndef ORACLE_TIMING
       if (epR[f] != recon_epoch && face_wet(FX(qpR, np, j, k), idx_u)) ++stale_wet_reads;
+#endif
       double lmin, lmax, rmin, rmax;
       eval_local_speeds_x(FX(qpL, np, j, k), gc_sx[f], lmin, lmax);
       eval_local_speeds_x(FX(qpR, np, j, k), gc_sx[f], rmin, rmax);
@@ -1357,8 +1375,12 @@ void OracleCtx::eval_speeds() {
     for (int64_t l = 0; l < solve_interfaces_y; ++l) {
       int j = j_stag_y[l], k = k_stag_y[l];
       size_t f = sy2(j, k);
+#ifndef ORACLE_TIMING
       if (epB[f] != recon_epoch && face_wet(FY(qpB, np, j, k), idx_v)) ++stale_wet_reads;
+#endif
+#ifndef ORACLE_TIMING
       if (epT[f] != recon_epoch && face_wet(FY(qpT, np, j, k), idx_v)) ++stale_wet_reads;
+#endif
       double bmin, bmax, tmin, tmax;
       eval_local_speeds_y(FY(qpB, np, j, k), gc_sy[f], bmin, bmax);
       eval_local_speeds_y(FY(qpT, np, j, k), gc_sy[f], tmin, tmax);
@@ -1478,6 +1500,26 @@ void OracleCtx::eval_hyperbolic_terms(int irk) {
       if (ny > 1) d[i] = d[i] + (FY(Hy, nv, j, k + 1)[i] - FY(Hy, nv, j, k)[i]) * one_by_dy;
     }
   }
+  // mass budget: SUM over solved cells of divFlux(1) written as the flux
+  // through the faces that have exactly one solved side (interior faces
+  // cancel); a cell outside the domain counts as not solved
+  auto solved = [&](int jj, int kk) {
+    return jj >= 1 && jj <= nx && kk >= 1 && kk <= ny && mask[c2(jj, kk)] != 0;
+  };
+  long double f = 0.0L;
+  if (nx > 1)
+    for (int64_t l = 0; l < solve_interfaces_x; ++l) {
+      int j = j_stag_x[l], k = k_stag_x[l];
+      int w = (int)solved(j - 1, k) - (int)solved(j, k);
+      if (w) f += (long double)w * FX(Hx, nv, j, k)[0] * (long double)one_by_dx;
+    }
+  if (ny > 1)
+    for (int64_t l = 0; l < solve_interfaces_y; ++l) {
+      int j = j_stag_y[l], k = k_stag_y[l];
+      int w = (int)solved(j, k - 1) - (int)solved(j, k);
+      if (w) f += (long double)w * FY(Hy, nv, j, k)[0] * (long double)one_by_dy;
+    }
+  stage_face_flux[irk - 1] = f;
 }
 
 // src/solver_2d.f90:872-1005
@@ -1753,6 +1795,7 @@ int OracleCtx::solve_rk_step(double* qj, const double* qj_old, double a_diag,
 // src/solver_2d.f90:1021-1632
 uint32_t OracleCtx::imex_RK_solver(double dtl) {
   const double T_amb = p.T_ambient;
+#pragma omp parallel for schedule(static)
   for (int64_t l = 0; l < solve_cells; ++l) {
     int j = j_cent[l], k = k_cent[l];
     std::memcpy(Q(q0, j, k), Q(q, j, k), sizeof(double) * nv);
@@ -1891,6 +1934,18 @@ uint32_t OracleCtx::imex_RK_solver(double dtl) {
   for (int m = 0; m < nrk; ++m) s2 += std::fabs(omega[m] - a_dirk_ij[nrk - 1][m]);
   const bool last_stage = (s1 == 0.0 && s2 == 0.0);
   uint32_t err = 0;
+  {
+    // mass budget: q(1) changes by -dt * SUM_m w_m * (face flux of stage m)
+    long double fl = 0.0L;
+    for (int m = 1; m <= nrk; ++m) {
+      const double w = last_stage ? a_tilde_ij[nrk - 1][m - 1] : omega_tilde[m - 1];
+      if (w != 0.0) fl += (long double)w * stage_face_flux[m - 1];
+    }
+    mass_budget[3] = -(long double)dtl * fl;
+    mass_budget[0] += mass_budget[3];
+  }
+  long double fix_before = 0.0L, fix_after = 0.0L;
+#pragma omp parallel for schedule(static) reduction(+ : fix_before, fix_after)
   for (int64_t l = 0; l < solve_cells; ++l) {
     int j = j_cent[l], k = k_cent[l];
     size_t cc = c2(j, k);
@@ -1909,6 +1964,7 @@ uint32_t OracleCtx::imex_RK_solver(double dtl) {
         qc[i] = q0c[i] - dtl * (sa - sb);
       }
     }
+    fix_before += qc[0];
     bool anynan = false;
     for (int i = 0; i < nv; ++i) anynan |= std::isnan(qc[i]);
     if (anynan) record_error(IMEX_ENAN, j, k);
@@ -1954,7 +2010,9 @@ uint32_t OracleCtx::imex_RK_solver(double dtl) {
     }
     if (!B_nodata.empty() && B_nodata[cc])
       for (int i = 0; i < nv; ++i) qc[i] = 0.0;
+    fix_after += qc[0];
   }
+  mass_budget[1] += fix_after - fix_before;
   (void)err;
   return error_mask;
 }
@@ -1963,12 +2021,15 @@ uint32_t OracleCtx::imex_RK_solver(double dtl) {
 uint32_t OracleCtx::update_erosion_deposition_cell(double dtl) {
   if (p.erosion_coeff == 0.0 && !p.settling_flag && !p.entrainment_flag) return 0;
   uint32_t err_all = 0;
+  long double ex_before = 0.0L, ex_after = 0.0L;
+#pragma omp parallel for schedule(static) reduction(+ : ex_before, ex_after) reduction(| : err_all)
   for (int64_t l = 0; l < solve_cells; ++l) {
     int j = j_cent[l], k = k_cent[l];
     size_t cc = c2(j, k);
     double* qc = Q(q, j, k);
     double* qpc = QP(qp, j, k);
     double pd;
+    ex_before += qc[0];
     if (qc[0] > 0.0) {
       qc_to_qp(qc, qpc, pd);
     } else {
@@ -2035,7 +2096,9 @@ uint32_t OracleCtx::update_erosion_deposition_cell(double dtl) {
       for (int i = 0; i < nv; ++i) qc[i] = 0.0;
     if (err) record_error(IMEX_EEROSION, j, k);
     err_all |= err;
+    ex_after += qc[0];
   }
+  mass_budget[2] += ex_after - ex_before;
   return err_all;
 }
 
@@ -2045,6 +2108,7 @@ void OracleCtx::post_step_sweep() {
     for (int64_t l = 0; l < solve_cells; ++l) post_cell(j_cent[l], k_cent[l], false);
     return;
   }
+#pragma omp parallel for schedule(static)
   for (int64_t l = 0; l < solve_cells; ++l) {
     int j = j_cent[l], k = k_cent[l];
     double pd;
@@ -2360,6 +2424,7 @@ void oracle_destroy(OracleCtx* o) { delete o; }
 
 void oracle_set_state(OracleCtx* o, const double* q, double t) {
   std::memcpy(o->q.data(), q, o->q.size() * sizeof(double));
+  for (int i = 0; i < 4; ++i) o->mass_budget[i] = 0.0L;
   o->t = t;
   o->check_solve(true, t);
   o->initial_sweep();
@@ -2467,6 +2532,10 @@ void oracle_stats(OracleCtx* o, ImexStats* st) {
 }
 
 int64_t oracle_stale_wet_reads(OracleCtx* o) { return o->stale_wet_reads; }
+
+void oracle_mass_budget(OracleCtx* o, double* out) {
+  for (int i = 0; i < 4; ++i) out[i] = (double)o->mass_budget[i];
+}
 
 void oracle_set_threads(int n) {
 #ifdef _OPENMP

@@ -50,6 +50,14 @@ void oracle_stats(OracleCtx* o, ImexStats* st);
  * earlier step and belong to a cell that was wet then (the reference's
  * arrays are never cleared between steps) */
 int64_t oracle_stale_wet_reads(OracleCtx* o);
+/* Changes of SUM(q(1,:,:)) since set_state by cause (multiply by dx*dy for
+ * mass): out[0] the fluxes through faces with exactly one solved side
+ * (domain border and inlet ring), computed from the face fluxes alone, so
+ * that SUM(q1) - SUM(q1 at set_state) - out[0] - out[1] - out[2] vanishes to
+ * round-off only if every interior face flux enters both of its cells;
+ * out[1] the assembly fixes (small negative h zeroed, no-data cells);
+ * out[2] the erosion/deposition update; out[3] out[0] of the last step. */
+void oracle_mass_budget(OracleCtx* o, double* out);
 void oracle_set_threads(int n);
 int oracle_max_threads(void);
 

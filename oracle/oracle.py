@@ -14,21 +14,40 @@ import numpy as np
 from imex_sflow2d_v2_b200.abi import ImexParams, ImexStatic, ImexStats, make_static
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB = None
+_LIBS = {}
+CHECKER = "liboracle.so"
+TIMING = "liboracle_timing.so"
 
 
-def build(force=False):
-    so = os.path.join(_HERE, "liboracle.so")
+def build(force=False, target=CHECKER):
+    so = os.path.join(_HERE, target)
     src = os.path.join(_HERE, "imex_oracle.cpp")
     if force or not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(src):
-        subprocess.check_call(["make", "-s", "-C", _HERE, "CXX=g++"])
+        subprocess.check_call(["make", "-s", "-C", _HERE, "CXX=g++", target])
     return so
 
 
-def lib():
-    global _LIB
-    if _LIB is None:
-        so = build()
+def timing_build_usable():
+    """The timing build targets x86-64-v3 (AVX2, FMA, BMI2): usable when the
+    host CPU reports those flags."""
+    try:
+        flags = set()
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    flags = set(line.split(":", 1)[1].split())
+                    break
+        return {"avx2", "fma", "bmi2", "movbe"} <= flags
+    except OSError:
+        return False
+
+
+def lib(target=CHECKER):
+    """ctypes handle of the checker build (default) or of the timing build
+    (TIMING: contraction on, instrument off; for the CPU baseline only)."""
+    L = _LIBS.get(target)
+    if L is None:
+        so = build(target=target)
         L = C.CDLL(so)
         vp = C.c_void_p
         dp = C.POINTER(C.c_double)
@@ -55,6 +74,7 @@ def lib():
         L.oracle_stats.argtypes = [vp, C.POINTER(ImexStats)]
         L.oracle_stale_wet_reads.restype = C.c_int64
         L.oracle_stale_wet_reads.argtypes = [vp]
+        L.oracle_mass_budget.argtypes = [vp, dp]
         L.oracle_set_threads.argtypes = [C.c_int]
         L.oracle_max_threads.restype = C.c_int
         L.oracle_qc_to_qp.argtypes = [vp, dp, dp]
@@ -81,8 +101,8 @@ def lib():
         L.oracle_output_prep.argtypes = [vp, C.c_int, C.c_int, C.c_int, dp, dp]
         L.oracle_limit.restype = C.c_double
         L.oracle_limit.argtypes = [C.c_double] * 6 + [C.c_int, C.c_double]
-        _LIB = L
-    return _LIB
+        _LIBS[target] = L
+    return L
 
 
 def _p(a):
@@ -92,8 +112,9 @@ def _p(a):
 class Oracle:
     """One oracle context; arrays use the Fortran layouts of imex_gpu.h."""
 
-    def __init__(self, params, static_arrays, threads=None):
-        L = lib()
+    def __init__(self, params, static_arrays, threads=None, timing=False):
+        L = lib(TIMING if timing else CHECKER)
+        self._L = L
         if threads is not None:
             L.oracle_set_threads(int(threads))
         self.params = params
@@ -105,17 +126,17 @@ class Oracle:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            lib().oracle_destroy(h)
+            self._L.oracle_destroy(h)
             self._h = None
 
     def set_state(self, q, t=0.0):
         q = np.ascontiguousarray(np.asarray(q, dtype=np.float64).ravel(order="F"))
-        lib().oracle_set_state(self._h, _p(q), float(t))
+        self._L.oracle_set_state(self._h, _p(q), float(t))
 
     def get_state(self, with_qp=False):
         q = np.zeros(self.nv * self.nx * self.ny)
         qp = np.zeros((self.nv + 2) * self.nx * self.ny) if with_qp else None
-        lib().oracle_get_state(self._h, _p(q), _p(qp) if with_qp else None)
+        self._L.oracle_get_state(self._h, _p(q), _p(qp) if with_qp else None)
         q = q.reshape((self.nv, self.nx, self.ny), order="F")
         if with_qp:
             return q, qp.reshape((self.nv + 2, self.nx, self.ny), order="F")
@@ -127,26 +148,26 @@ class Oracle:
         de = np.zeros(self.ns * n)
         eo = np.zeros(self.ns * n)
         B = np.zeros(n)
-        lib().oracle_get_exchange(self._h, _p(er), _p(de), _p(eo), _p(B))
+        self._L.oracle_get_exchange(self._h, _p(er), _p(de), _p(eo), _p(B))
         return (er.reshape((self.ns, self.nx, self.ny), order="F"),
                 de.reshape((self.nx, self.ny, self.ns), order="F"),
                 eo.reshape((self.nx, self.ny, self.ns), order="F"),
                 B.reshape((self.nx, self.ny), order="F"))
 
     def check_solve(self, t, solve_all=False):
-        return lib().oracle_check_solve(self._h, float(t), int(solve_all))
+        return self._L.oracle_check_solve(self._h, float(t), int(solve_all))
 
     def timestep(self):
-        return lib().oracle_timestep(self._h)
+        return self._L.oracle_timestep(self._h)
 
     def rk_step(self, t, dt):
-        return lib().oracle_rk_step(self._h, float(t), float(dt))
+        return self._L.oracle_rk_step(self._h, float(t), float(dt))
 
     def erosion_deposition(self, dt):
-        return lib().oracle_erosion_deposition(self._h, float(dt))
+        return self._L.oracle_erosion_deposition(self._h, float(dt))
 
     def post_step(self):
-        lib().oracle_post_step(self._h)
+        self._L.oracle_post_step(self._h)
 
     def get_masks(self):
         nx, ny = self.nx, self.ny
@@ -154,26 +175,34 @@ class Oracle:
         mx = np.zeros((nx + 1) * ny, np.int8)
         my = np.zeros(nx * (ny + 1), np.int8)
         i8 = C.POINTER(C.c_int8)
-        lib().oracle_get_masks(self._h, m.ctypes.data_as(i8), mx.ctypes.data_as(i8),
+        self._L.oracle_get_masks(self._h, m.ctypes.data_as(i8), mx.ctypes.data_as(i8),
                                my.ctypes.data_as(i8))
         return (m.reshape((nx, ny), order="F"), mx.reshape((nx + 1, ny), order="F"),
                 my.reshape((nx, ny + 1), order="F"))
 
     def set_clock(self, t, dt0, t_end=1e300, t_output=-1.0):
-        lib().oracle_set_clock(self._h, float(t), float(dt0), float(t_end), float(t_output))
+        self._L.oracle_set_clock(self._h, float(t), float(dt0), float(t_end), float(t_output))
 
     def advance(self, n_steps):
         t = C.c_double(0.0)
-        err = lib().oracle_advance(self._h, int(n_steps), C.byref(t))
+        err = self._L.oracle_advance(self._h, int(n_steps), C.byref(t))
         return err, t.value
 
     def stats(self):
         s = ImexStats()
-        lib().oracle_stats(self._h, C.byref(s))
+        self._L.oracle_stats(self._h, C.byref(s))
         return s
 
     def stale_wet_reads(self):
-        return lib().oracle_stale_wet_reads(self._h)
+        return self._L.oracle_stale_wet_reads(self._h)
+
+    def mass_budget(self):
+        """Changes of SUM(q1) since set_state by cause: (border and inlet face
+        fluxes, assembly fixes, erosion/deposition, face fluxes of the last
+        step); multiply by dx*dy for mass."""
+        out = np.zeros(4)
+        self._L.oracle_mass_budget(self._h, out.ctypes.data_as(C.POINTER(C.c_double)))
+        return tuple(float(x) for x in out)
 
     # the driver's output sweep
     def post_init(self, thickness_levels=(), dyn_pres_levels=()):
@@ -182,7 +211,7 @@ class Oracle:
         self._nt = len(t) * len(d)
         t = np.ascontiguousarray(t, dtype=np.float64)
         d = np.ascontiguousarray(d, dtype=np.float64)
-        lib().oracle_post_init(self._h, len(t), _p(t), len(d), _p(d))
+        self._L.oracle_post_init(self._h, len(t), _p(t), len(d), _p(d))
 
     def output_prep(self, cons, phys, esri):
         """(p2d (17+4ns, nx, ny), esr (2, nx, ny)) of output_solution, with its
@@ -190,45 +219,45 @@ class Oracle:
         nx, ny, ns = self.nx, self.ny, self.ns
         p2d = np.zeros((17 + 4 * ns) * nx * ny)
         esr = np.zeros(2 * nx * ny)
-        lib().oracle_output_prep(self._h, int(cons), int(phys), int(esri), _p(p2d), _p(esr))
+        self._L.oracle_output_prep(self._h, int(cons), int(phys), int(esri), _p(p2d), _p(esr))
         return (p2d.reshape(17 + 4 * ns, ny, nx).transpose(0, 2, 1),
                 esr.reshape(2, ny, nx).transpose(0, 2, 1))
 
     def post_diag(self):
         out = np.zeros(4)
-        lib().oracle_post_diag(self._h, _p(out))
+        self._L.oracle_post_diag(self._h, _p(out))
         return tuple(out)
 
     def get_post(self):
         n = self.nx * self.ny
         a = [np.zeros(n) for _ in range(3)]
         v = np.zeros(max(self._nt, 1) * n, np.int8)
-        lib().oracle_get_post(self._h, _p(a[0]), _p(a[1]), _p(a[2]),
+        self._L.oracle_get_post(self._h, _p(a[0]), _p(a[1]), _p(a[2]),
                               v.ctypes.data_as(C.POINTER(C.c_int8)))
         f = [x.reshape((self.nx, self.ny), order="F") for x in a]
         return f[0], f[1], f[2], v[:self._nt * n].reshape((self._nt, self.nx, self.ny), order="F")
 
     def topography_reconstruction(self):
-        lib().oracle_topography_reconstruction(self._h)
+        self._L.oracle_topography_reconstruction(self._h)
 
     def get_topo(self):
         """B_prime_x/y_geom, B_second_xx/xy/yy_geom, grav_coeff, d_grav_coeff_dx."""
         n = self.nx * self.ny
         a = [np.zeros(n) for _ in range(7)]
-        lib().oracle_get_topo(self._h, *[_p(x) for x in a])
+        self._L.oracle_get_topo(self._h, *[_p(x) for x in a])
         return [x.reshape((self.nx, self.ny), order="F") for x in a]
 
     # point functions
     def qc_to_qp(self, qc):
         qc = np.ascontiguousarray(qc, dtype=np.float64)
         out = np.zeros(self.nv + 2)
-        lib().oracle_qc_to_qp(self._h, _p(qc), _p(out))
+        self._L.oracle_qc_to_qp(self._h, _p(qc), _p(out))
         return out
 
     def qp_to_qc(self, qp):
         qp = np.ascontiguousarray(qp, dtype=np.float64)
         out = np.zeros(self.nv)
-        lib().oracle_qp_to_qc(self._h, _p(qp), _p(out))
+        self._L.oracle_qp_to_qc(self._h, _p(qp), _p(out))
         return out
 
     def implicit_terms(self, q_re, q_im=None):
@@ -236,7 +265,7 @@ class Oracle:
         q_im = None if q_im is None else np.ascontiguousarray(q_im, dtype=np.float64)
         re = np.zeros(self.nv)
         im = np.zeros(self.nv)
-        lib().oracle_implicit_terms(self._h, _p(q_re), _p(q_im) if q_im is not None else None,
+        self._L.oracle_implicit_terms(self._h, _p(q_re), _p(q_im) if q_im is not None else None,
                                     _p(re), _p(im))
         return re, im
 
@@ -244,7 +273,7 @@ class Oracle:
         qj = np.array(qj, dtype=np.float64)
         qo = np.ascontiguousarray(qj_old, dtype=np.float64)
         rj = np.ascontiguousarray(rj, dtype=np.float64)
-        it = lib().oracle_solve_rk_step(self._h, _p(qj), _p(qo), _p(rj), float(bx), float(by),
+        it = self._L.oracle_solve_rk_step(self._h, _p(qj), _p(qo), _p(rj), float(bx), float(by),
                                         float(dt), float(a_diag))
         return qj, it
 

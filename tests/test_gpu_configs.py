@@ -1,0 +1,114 @@
+"""The workloads the throughput figures are quoted on, at their stated sizes,
+against the oracle through the C ABI.
+
+Acceptance: solve masks bit for bit after every compared step, the same
+dt/t, every conserved variable bit for bit (which implies relative L1 <=
+1e-10; that bound is asserted as well), no read of an earlier step's values
+in the oracle, the same reference checks, and total mass conserved to
+round-off: the change of dx*dy*SUM(q1) of the GPU state equals the mass
+carried through the domain border and the inlet ring (computed by the
+oracle from its face fluxes alone) plus the assembly fixes and the
+erosion/deposition exchange, to a relative 1e-12.
+
+  dam break          200x200 cells of 0.05 m, 500 steps, every step compared
+  radial current     1024x1024 cells of 2 m, two solid classes, Voellmy,
+                     2000 steps through advance() replayed from a CUDA graph
+  fractal inlet      512x512 instance of the 4096^2 workload's generator
+                     (three classes, settling + erosion, 2 m layer), 60 steps
+"""
+import math
+
+import numpy as np
+import pytest
+
+from imex_sflow2d_v2_b200 import configs
+from imex_sflow2d_v2_b200.solver import ImexSolver
+from oracle import Oracle
+from parity import lockstep, rel_l1
+
+pytestmark = pytest.mark.gpu
+
+REL_L1_TOL = 1e-10     # conserved variables
+MASS_TOL = 1e-12       # relative closure of the mass budget
+
+
+def q1_sum(q):
+    return math.fsum(np.asarray(q[0]).ravel().tolist())
+
+
+def budget_residual(o, q_gpu, m0):
+    """(SUM q1 now - SUM q1 at start - budget) / SUM q1 now."""
+    b = o.mass_budget()
+    m = q1_sum(q_gpu)
+    return (m - m0 - b[0] - b[1] - b[2]) / max(abs(m), 1e-300)
+
+
+def test_dambreak_200_500_steps_lockstep():
+    p, st, q = configs.dambreak()
+    assert (p.nx, p.ny, p.cell_size) == (200, 200, 0.05)
+    recs, o, g = lockstep(p, st, q, 500, threads=None, mass=True)
+    for r in recs:
+        assert r["stale"] == 0, r
+        assert r["cells"][0] == r["cells"][1], r
+        assert r["mask_equal"], r
+        assert r["dt"][0] == r["dt"][1], r
+        assert r["q_equal"], r
+        assert r["rel_l1"] <= REL_L1_TOL, r
+        assert r["err"][0] == r["err"][1], r
+        assert r["err"][0][0] == 0, r
+        assert abs(r["mass_resid"]) <= MASS_TOL, r
+    # the front has reached the transmissive borders: mass has left
+    assert o.mass_budget()[0] < 0.0
+
+
+def _advance_compare(p, st, q, total, chunk, use_graph, exchange=False):
+    o = Oracle(p, st)
+    g = ImexSolver(p, st)
+    for x in (o, g):
+        x.set_state(q, 0.0)
+        x.set_clock(0.0, 1e-2)
+    m0 = q1_sum(q)
+    done = 0
+    worst = 0.0
+    while done < total:
+        n = min(chunk, total - done)
+        eo, to = o.advance(n)
+        rc, tg = g.advance(n, use_graph=use_graph)
+        done += n
+        assert tg == to, done
+        qo, qg = o.get_state(), g.get_state()
+        assert np.array_equal(qo, qg), (done, float(np.abs(qo - qg).max()))
+        assert rel_l1(qo, qg) <= REL_L1_TOL
+        for a, b in zip(o.get_masks(), g.get_masks()):
+            assert np.array_equal(a, b), done
+        so, sg = o.stats(), g.stats()
+        assert (so.error_mask, so.first_error_code, so.first_error_j, so.first_error_k) == \
+            (sg.error_mask, sg.first_error_code, sg.first_error_j, sg.first_error_k), done
+        assert so.error_mask == 0, done
+        assert (so.newton_cells, so.newton_iters, so.lnsrch_trials) == \
+            (sg.newton_cells, sg.newton_iters, sg.lnsrch_trials), done
+        assert o.stale_wet_reads() == 0, done
+        if exchange:
+            for a, b in zip(o.get_exchange(), g.get_exchange()):
+                assert np.array_equal(a, b), done
+        r = budget_residual(o, qg, m0)
+        worst = max(worst, abs(r))
+        assert abs(r) <= MASS_TOL, (done, r)
+    return o, g, worst
+
+
+def test_radial_current_1024_2000_steps():
+    p, st, q = configs.radial_current()
+    assert (p.nx, p.ny, p.n_solid, p.cell_size) == (1024, 1024, 2, 2.0)
+    o, g, worst = _advance_compare(p, st, q, 2000, 250, use_graph=True)
+    # the inlet has fed the current: the budget is dominated by the inflow
+    assert o.mass_budget()[0] > 0.0
+    assert g.stats().solve_cells > 100000
+
+
+def test_fractal_inlet_512_60_steps():
+    p, st, q = configs.fractal_inlet(n=512, initial_layer=2.0)
+    assert (p.nx, p.n_solid, p.settling_flag) == (512, 3, 1) and p.erosion_coeff > 0.0
+    o, g, worst = _advance_compare(p, st, q, 60, 10, use_graph=False, exchange=True)
+    b = o.mass_budget()
+    assert b[2] != 0.0        # erosion/deposition moved mass

@@ -49,3 +49,24 @@ def test_noalloc_dt_radial_then_dambreak():
 def test_noalloc_dt_fractal():
     p, st, q = cases.fractal_small()
     _walk(p, st, q, 6)
+
+
+def test_noalloc_allocates_no_device_memory():
+    """The entry point's defining property: once the first call on the
+    device has resolved the scratch array's address (and the kernels are
+    loaded), further calls leave the device's free memory unchanged."""
+    import torch
+    p, st, q = cases.radial(n=64)
+    g = ImexSolver(p, st)
+    g.set_state(q, 0.0)
+    g.check_solve(0.0)
+    d0 = g.timestep()
+    g.timestep_noalloc()
+    g.sync()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(20):
+        assert _close(g.timestep_noalloc(), d0)
+    g.sync()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    g.close()
