@@ -38,6 +38,7 @@ METRIC = "FP64 cell-updates/s (4096² grid); Newton iters/cell, learned vs plain
 UNIT = "cell-updates/s"
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
+BUILD_MODE = "exact"   # the headline build; fast mode is measured beside it
 
 
 def parse():
@@ -62,6 +63,10 @@ def parse():
                     help="grid side of the output measurement (0 = skip)")
     ap.add_argument("--learned-pairs", type=int, default=10_000_000)
     ap.add_argument("--learned-n", type=int, default=1024, help="side of the comparison grid")
+    ap.add_argument("--parity-steps", type=int, default=10,
+                    help="steps of the GPU-vs-oracle check on the CPU sample (0 = skip)")
+    ap.add_argument("--no-config-rates", action="store_true")
+    ap.add_argument("--no-fast", action="store_true", help="skip the fast-mode measurement")
     return ap.parse_args()
 
 
@@ -98,7 +103,8 @@ def bytes_per_cell(ns, erosion, listed=(1.0, 0.0, 0.0)):
 
 def fp64_counts():
     """FP64 instructions (DADD+DMUL+DFMA, per thread) per cell of each kernel
-    group, from the ncu capture summarised in profiles/fp64_inst_per_cell.json."""
+    group and build ("exact", "fast"), from the ncu captures summarised in
+    profiles/fp64_inst_per_cell.json."""
     try:
         return json.load(open(os.path.join(ROOT, "profiles", "fp64_inst_per_cell.json")))
     except Exception:
@@ -162,31 +168,133 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(args, threads=None):
-    """The CPU oracle on a bounded sample of the workload."""
+def cpu_info():
+    """Host CPU model, logical CPUs and the vector flags the timing build uses."""
+    model, flags = "unknown", set()
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name") and model == "unknown":
+                    model = line.split(":", 1)[1].strip()
+                elif line.startswith("flags") and not flags:
+                    flags = set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    keep = [x for x in ("avx2", "fma", "avx512f", "amx_tile") if x in flags]
+    return {"model": model, "logical_cpus": os.cpu_count(), "flags": keep}
+
+
+def _time_oracle(args, p, st, q, threads, timing, budget_s):
+    """Cell-updates/s of the oracle on (p, st, q): one untimed step, then
+    enough steps for about `budget_s` seconds (at least one)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
-    orc.build()
-    p, st, q = workload(args.cpu_n, args.layer)
-    o = orc.Oracle(p, st, threads=threads)
+    o = orc.Oracle(p, st, threads=threads, timing=timing)
     o.set_state(q, 0.0)
     o.set_clock(0.0, 1e-2)
-    o.advance(1)  # first step outside the timing (page-in)
-    steps = args.cpu_steps
-    if steps <= 0:
-        t0 = time.perf_counter()
-        o.advance(1)
-        one = time.perf_counter() - t0
-        steps = max(1, min(50, int(15.0 / max(one, 1e-3))))
+    t0 = time.perf_counter()
+    o.advance(1)                       # page-in, thread start-up
+    one = time.perf_counter() - t0
+    steps = args.cpu_steps if args.cpu_steps > 0 else max(1, min(50, int(budget_s / max(one, 1e-3))))
     t0 = time.perf_counter()
     o.advance(steps)
     el = time.perf_counter() - t0
-    cells = args.cpu_n * args.cpu_n
-    cores = orc.lib().oracle_max_threads() if threads is None else threads
-    return {"value": cells * steps / el, "unit": UNIT, "cores": int(cores), "kind": "port",
-            "sample": "%dx%d instance of the same generator (seed, physics, 2 m layer), "
-                      "%d steps after 2 untimed, %.1f s, OpenMP %d threads"
-                      % (args.cpu_n, args.cpu_n, steps, el, cores, )}
+    return p.nx * p.ny * steps / el, steps, el
+
+
+def cpu_baseline(args, single_thread=True):
+    """The oracle's timing build (-O3, x86-64-v3, contraction on, stale-read
+    instrument off; the checker build if this CPU lacks AVX2/FMA) on a
+    bounded sample of the workload: the same generator at --cpu-n, with all
+    host threads and with one.  Its OpenMP loops are the reference's
+    (assembly, erosion/deposition, reconstruction, fluxes, Newton)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    timing = orc.timing_build_usable()
+    orc.build(target=orc.TIMING if timing else orc.CHECKER)
+    p, st, q = workload(args.cpu_n, args.layer)
+    cores = orc.lib(orc.TIMING if timing else orc.CHECKER).oracle_max_threads()
+    v_all, n_all, el_all = _time_oracle(args, p, st, q, cores, timing, 15.0)
+    out = {"value": v_all, "unit": UNIT, "cores": int(cores), "kind": "port",
+           "build": ("oracle timing build: g++ -O3 -march=x86-64-v3 -ffp-contract=fast, "
+                     "instrument off" if timing else "oracle checker build: g++ -O2 "
+                     "-ffp-contract=off (no AVX2/FMA on this CPU)"),
+           "sample": "%dx%d instance of the same generator (seed, physics, 2 m layer), "
+                     "%d steps after 1 untimed, %.1f s, OpenMP %d threads"
+                     % (args.cpu_n, args.cpu_n, n_all, el_all, cores),
+           "threads_all": {"threads": int(cores), "value": v_all, "steps": n_all,
+                           "seconds": el_all},
+           "cpu": cpu_info()}
+    if single_thread:
+        v1, n1, el1 = _time_oracle(args, p, st, q, 1, timing, 12.0)
+        out["threads_1"] = {"threads": 1, "value": v1, "steps": n1, "seconds": el1}
+    return out
+
+
+def cpu_parity(args, device):
+    """The GPU path against the oracle's checker build on the CPU baseline's
+    sample (same instance, same steps through advance): masks, t and every
+    conserved variable after the steps."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    from imex_sflow2d_v2_b200.solver import ImexSolver
+    p, st, q = workload(args.cpu_n, args.layer)
+    steps = args.parity_steps
+    o = orc.Oracle(p, st, threads=orc.lib().oracle_max_threads())
+    g = ImexSolver(p, st, device=device)
+    for x in (o, g):
+        x.set_state(q, 0.0)
+        x.set_clock(0.0, 1e-2)
+    _, to = o.advance(steps)
+    _, tg = g.advance(steps)
+    qo, qg = o.get_state(), g.get_state()
+    masks = all(np.array_equal(a, b) for a, b in zip(o.get_masks(), g.get_masks()))
+    den = float(np.abs(qo).sum())
+    rl1 = float(np.abs(qo - qg).sum()) / den if den > 0 else float(np.abs(qo - qg).sum())
+    ex = all(np.array_equal(a, b) for a, b in zip(o.get_exchange(), g.get_exchange()))
+    so, sg = o.stats(), g.stats()
+    g.close()
+    return {"workload": "%dx%d instance of the benchmark generator" % (args.cpu_n, args.cpu_n),
+            "steps": steps, "masks_equal": bool(masks), "q_equal": bool(np.array_equal(qo, qg)),
+            "exchange_equal": bool(ex), "rel_l1": rl1, "t_equal": bool(to == tg),
+            "newton_iters_equal": bool(so.newton_iters == sg.newton_iters),
+            "stale_wet_reads": int(o.stale_wet_reads()), "tolerance_rel_l1": 1e-10}
+
+
+def config_rates(args, device):
+    """Cell-updates/s of the first two workloads at their stated sizes and
+    step counts, each run from its initial state through advance() replayed
+    from a CUDA graph (device time by CUDA events on the library's stream)."""
+    import torch
+    from imex_sflow2d_v2_b200 import configs
+    from imex_sflow2d_v2_b200.solver import ImexSolver
+    out = {}
+    for name, (p, st, q), steps in (
+            ("dambreak_200", configs.dambreak(), 500),
+            ("radial_current_1024", configs.radial_current(), 2000)):
+        g = ImexSolver(p, st, device=device)
+        stream = torch.cuda.current_stream()
+        g.set_stream(stream.cuda_stream)
+        g.set_state(q, 0.0)
+        g.set_clock(0.0, 1e-2)
+        g.sync()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        cells = 0
+        ev0.record(stream)
+        for chunk in range(0, steps, 100):
+            g.advance(min(100, steps - chunk), use_graph=True)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        s_ = g.stats()
+        out[name] = {"grid": [p.nx, p.ny], "steps": steps,
+                     "value": p.nx * p.ny * steps / (ms * 1e-3), "unit": UNIT,
+                     "ms_per_step": ms / steps, "solve_cells_last_step": int(s_.solve_cells),
+                     "t_end": s_.t, "errors": int(s_.error_mask)}
+        g.close()
+    return out
 
 
 def run_ensemble(args):
@@ -385,10 +493,50 @@ def run_learned(args, g, p):
             "rel_l1_learned_vs_plain_after_20_steps": diff}
 
 
+def run_fast(args, p, st, q0, device, cells, g_exact):
+    """Fast mode (contracted multiply-adds) on the headline workload: its
+    device-timed rate over the same warm-up and timed steps, and its state,
+    masks and clock after those steps against the exact mode's (`g_exact`,
+    which ran the same steps from the same state)."""
+    import numpy as np
+    import torch
+    from imex_sflow2d_v2_b200.solver import ImexSolver
+    gf = ImexSolver(p, st, device=device, fast=True)
+    stream = torch.cuda.current_stream()
+    gf.set_stream(stream.cuda_stream)
+    gf.set_state(q0, 0.0)
+    gf.set_clock(0.0, 1e-2)
+    for _ in range(args.warmup):
+        gf.advance(1)
+    gf.sync()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        gf.advance(1)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    qf, qe = gf.get_state(), g_exact.get_state()
+    masks = all(np.array_equal(a, b) for a, b in zip(gf.get_masks(), g_exact.get_masks()))
+    den = float(np.abs(qe).sum())
+    rl1 = float(np.abs(qf - qe).sum()) / den if den > 0 else 0.0
+    tf, te = gf.stats().t, g_exact.stats().t
+    info = gf.lib.imex_gpu_build_info().decode()
+    gf.close()
+    return {"value": cells * args.steps / (ms * 1e-3), "unit": UNIT,
+            "ms_per_step": ms / args.steps, "build": info,
+            "compared_after_steps": args.warmup + args.steps,
+            "masks_equal": bool(masks), "rel_l1_vs_exact": rl1,
+            "t_rel_diff": abs(tf - te) / max(abs(te), 1e-300),
+            "tolerance_rel_l1": 1e-10}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    cb = cpu_baseline(args)
+    cb = cpu_baseline(args, single_thread=False)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -401,8 +549,38 @@ def run_reference(args, rank, world):
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
             "note": "the reference is Fortran; no Fortran compiler in this image, so its "
-                    "C++ restatement (the oracle) is timed"}
+                    "C++ restatement (the oracle, timing build, the reference's OpenMP "
+                    "loops) is timed"}
     print(json.dumps(line), flush=True)
+
+
+def roofline_line(dom, fp64, achieved, peak, peak_src, traffic, alg_bytes, avg_s, timed,
+                  steps_timed, fp64_peak, hbm_frac_s8d, s8d_bytes):
+    """The dominant kernel group's roofline.  Flux, Newton and erosion are
+    bound by dependent FP64 arithmetic, so their headline fraction is the
+    FP64-pipe one; the HBM figures stay beside it: `achieved`/`frac_hbm` from
+    the split design's algorithmic bytes, `traffic` (ncu DRAM bytes per
+    launch, whose ratio to `alg_bytes_per_launch` measures re-reads and
+    spills) and `hbm_frac_s8d` (the whole step against the fused minimum of
+    `s8d_bytes_per_cell`)."""
+    fp64_bound = fp64 is not None and dom in ("flux", "stage2_first", "stage2_iter", "erosion")
+    line = {"kernel": dom,
+            "bound": "fp64" if fp64_bound else "hbm",
+            "achieved": fp64["achieved_inst_per_s"] / 1e12 if fp64_bound else achieved,
+            "peak": fp64["peak_inst_per_s"] / 1e12 if fp64_bound else peak,
+            "unit": "T FP64 inst/s" if fp64_bound else "GB/s",
+            "frac": fp64["frac"] if fp64_bound else achieved / peak,
+            "peak_source": ("measured FP64 FMA chain (k_fp64_probe)" if fp64_bound
+                            else peak_src),
+            "achieved_hbm_gbs": achieved, "peak_hbm_gbs": peak, "peak_hbm_source": peak_src,
+            "frac_hbm": achieved / peak,
+            "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
+            "traffic_over_alg": (traffic / alg_bytes) if traffic else None,
+            "avg_launch_ms": avg_s * 1e3,
+            "kernel_ms_per_step": {k: v[0] / steps_timed for k, v in timed.items()},
+            "fp64_pipe": fp64, "fp64_fma_peak_gflops": fp64_peak,
+            "hbm_frac_s8d": hbm_frac_s8d, "s8d_bytes_per_cell": s8d_bytes}
+    return line
 
 
 def main():
@@ -495,14 +673,25 @@ def main():
         pass
     # FP64 pipe: instructions per cell (ncu) x cells / live kernel time, against
     # the measured FMA-chain peak (one FP64 instruction per lane per FMA)
-    fpc = fp64_counts()
+    fpc = fp64_counts().get(BUILD_MODE, {})
     fp64 = None
-    if fp64_peak and dom in fpc:
-        inst_s = fpc[dom] * cells / avg_s
+    fp64_all = {}
+    if fp64_peak:
         peak_inst_s = fp64_peak * 1e9 / 2.0
-        fp64 = {"kernel": dom, "inst_per_cell": fpc[dom], "achieved_inst_per_s": inst_s,
-                "peak_inst_per_s": peak_inst_s, "frac": inst_s / peak_inst_s,
-                "peak_source": "measured FP64 FMA chain (k_fp64_probe)"}
+        for k_, (tot_ms, _) in timed.items():
+            if fpc.get(k_):
+                fp64_all[k_] = fpc[k_] * cells / (tot_ms / steps_timed * 1e-3) / peak_inst_s
+        if dom in fpc:
+            inst_s = fpc[dom] * cells / avg_s
+            fp64 = {"kernel": dom, "inst_per_cell": fpc[dom], "achieved_inst_per_s": inst_s,
+                    "peak_inst_per_s": peak_inst_s, "frac": inst_s / peak_inst_s,
+                    "peak_source": "measured FP64 FMA chain (k_fp64_probe)",
+                    "frac_per_kernel": fp64_all}
+    # the whole step against the HBM roofline of the fused minimum traffic:
+    # 8*(3*n_v + 2) + 1 bytes per cell plus 8*(3*n_s*2) for the erosion planes
+    nv_ = 4 + p.n_solid
+    s8d_bytes = 8 * (3 * nv_ + 2) + 1 + (8 * 3 * p.n_solid * 2 if erosion else 0)
+    hbm_frac_s8d = s8d_bytes * cells / (ms / args.steps * 1e-3) / 1e9 / peak
 
     # end to end through the public API with pinned host buffers
     e2e = None
@@ -526,6 +715,15 @@ def main():
                "h2d_bytes_per_step": nv * cells * 8, "d2h_bytes_per_step": nv * cells * 8,
                "steps": args.e2e_steps}
 
+    fast = None
+    if rank == 0 and world == 1 and not args.no_fast:
+        # the exact context ran warm-up + timed steps from q0; the e2e leg
+        # re-ran it from q0, so bring it to the same step count again
+        if not args.no_e2e:
+            g.set_state(q0, 0.0)
+            g.set_clock(0.0, 1e-2)
+            g.advance(args.warmup + args.steps)
+        fast = run_fast(args, p, st, q0, local, cells, g)
     learned = None
     if rank == 0 and world == 1 and not args.no_learned:
         learned = run_learned(args, g, p)
@@ -549,6 +747,15 @@ def main():
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(args)
+    parity = None
+    if rank == 0 and world == 1 and args.parity_steps > 0:
+        parity = cpu_parity(args, local)
+    rates = None
+    if rank == 0 and world == 1 and not args.no_config_rates:
+        rates = config_rates(args, local)
+        rates["fractal_inlet_%d" % n] = {"grid": [n, n], "steps": args.steps, "value": value,
+                                         "unit": UNIT, "ms_per_step": ms / args.steps,
+                                         "note": "the headline value (2 m initial layer)"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -565,15 +772,16 @@ def main():
             "lnsrch_trials_per_cell": s1.lnsrch_trials / ncells_newton,
             "gpu_launches": launches,
             "clocks": clocks,
-            "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
-                         "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
-                         "avg_launch_ms": avg_s * 1e3,
-                         "kernel_ms_per_step": {k: v[0] / steps_timed for k, v in timed.items()},
-                         "fp64_pipe": fp64, "fp64_fma_peak_gflops": fp64_peak},
+            "roofline": roofline_line(dom, fp64, achieved, peak, peak_src, traffic, alg_bytes,
+                                      avg_s, timed, steps_timed, fp64_peak, hbm_frac_s8d,
+                                      s8d_bytes),
             "e2e": e2e,
             "cpu_baseline": cb,
             "errors": int(s1.error_mask),
+            "build": BUILD_MODE,
+            "parity": parity,
+            "config_rates": rates,
+            "fast_mode": fast,
             "ensemble": ensemble,
             "learned_vs_plain": learned,
             "setup": setup,

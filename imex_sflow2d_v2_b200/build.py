@@ -1,4 +1,5 @@
-"""Build libimexgpu.so for sm_100a (nvcc; no GPU needed)."""
+"""Build libimexgpu.so (exact mode) and libimexgpu_fast.so (contracted
+multiply-adds) for sm_100a (nvcc; no GPU needed)."""
 import os
 import subprocess
 import sys
@@ -6,6 +7,7 @@ import sys
 _HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(_HERE, "csrc")
 LIB = os.path.join(_HERE, "libimexgpu.so")
+LIB_FAST = os.path.join(_HERE, "libimexgpu_fast.so")
 
 
 def sources():
@@ -17,15 +19,18 @@ def sources():
 
 
 def needs_build():
-    if not os.path.exists(LIB):
-        return True
-    t = os.path.getmtime(LIB)
-    return any(os.path.getmtime(s) > t for s in sources())
+    for lib in (LIB, LIB_FAST):
+        if not os.path.exists(lib):
+            return True
+        t = os.path.getmtime(lib)
+        if any(os.path.getmtime(s) > t for s in sources()):
+            return True
+    return False
 
 
 def build(force=False, verbose=False):
     if force or needs_build():
-        cmd = ["make", "-C", CSRC, "NVCC=/usr/local/cuda/bin/nvcc"]
+        cmd = ["make", "-j2", "-C", CSRC, "NVCC=/usr/local/cuda/bin/nvcc", "all"]
         if force:
             cmd.insert(1, "-B")
         out = subprocess.run(cmd, capture_output=not verbose, text=True)

@@ -102,6 +102,35 @@ def topography_geom(B, dx, dy):
     c1 = [-2.0, -1.0, 0.0, 1.0, 2.0]
     c2 = [2.0, -1.0, -2.0, -1.0, 2.0]
     out = {}
+    if (ny == 1 and nx >= 5) or (nx == 1 and ny >= 5):
+        # a one-row (one-column) grid.  The reference's stencil loop runs over
+        # rows 3..ny-2, none here, and its border copies then index rows 3,
+        # 0 and -1 of the one-row arrays (src/geometry_2d.f90:700-790), so
+        # its values are undefined; the planes below are the loop's stencil
+        # applied along the row, with the cross-direction terms zero
+        along_x = ny == 1
+        b = B[:, 0] if along_x else B[0, :]
+        n, d = len(b), (dx if along_x else dy)
+        p1 = np.zeros(n)
+        p2 = np.zeros(n)
+        for kj in range(5):
+            p1[2:n - 2] = p1[2:n - 2] + c1[kj] * b[kj:kj + n - 4]
+            p2[2:n - 2] = p2[2:n - 2] + c2[kj] * b[kj:kj + n - 4]
+        p1[2:n - 2] = p1[2:n - 2] / (10.0 * d)
+        p2[2:n - 2] = p2[2:n - 2] / (7.0 * d ** 2)
+        for a in (p1, p2):
+            a[0] = a[1] = a[2]
+            a[n - 1] = a[n - 2] = a[n - 3]
+        shape = B.shape
+        z = np.zeros(shape)
+        first = np.asfortranarray(p1.reshape(shape))
+        second = np.asfortranarray(p2.reshape(shape))
+        out["B_prime_x_geom"] = first if along_x else z.copy()
+        out["B_prime_y_geom"] = z.copy() if along_x else first
+        out["B_second_xx_geom"] = second if along_x else z.copy()
+        out["B_second_yy_geom"] = z.copy() if along_x else second
+        out["B_second_xy_geom"] = z.copy()
+        return out
     if nx < 5 or ny < 5:
         z = np.zeros((nx, ny))
         for n in ("B_prime_x_geom", "B_prime_y_geom", "B_second_xx_geom",

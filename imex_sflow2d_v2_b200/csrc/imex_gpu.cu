@@ -381,7 +381,7 @@ cudaError_t enqueue_step(ImexCtx* ctx) {
 
 int validate(const ImexParams* p, std::string& why) {
   if (p->abi_version != IMEX_ABI_VERSION) { why = "abi_version mismatch"; return IMEX_EINVAL; }
-  if (p->nx < 3 || p->ny < 3) { why = "grids with fewer than 3 cells per direction are not implemented"; return IMEX_EUNSUPPORTED; }
+  if (p->nx < 1 || p->ny < 1) { why = "nx and ny must be at least 1"; return IMEX_EINVAL; }
   if (p->n_solid < 1 || p->n_solid > IMEX_MAX_SOLID) { why = "n_solid out of range"; return IMEX_EINVAL; }
   if (p->n_rk != 2) { why = "only the n_RK=2 IMEX tableau is implemented"; return IMEX_EUNSUPPORTED; }
   if (!p->gas_flag || p->liquid_flag) { why = "only a gas carrier phase is implemented"; return IMEX_EUNSUPPORTED; }
@@ -412,7 +412,11 @@ int validate(const ImexParams* p, std::string& why) {
 extern "C" {
 
 const char* imex_gpu_build_info(void) {
+#ifdef IMEX_FMAD
+  return "imex_gpu sm_100a fmad=true prec-div prec-sqrt abi=1";
+#else
   return "imex_gpu sm_100a fmad=false prec-div prec-sqrt abi=1";
+#endif
 }
 
 const char* imex_gpu_last_error(ImexCtx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
@@ -449,9 +453,10 @@ int imex_gpu_create(const ImexParams* p, const ImexStatic* s, int device, ImexCt
   P.plane = P.pitch * P.ny;
   P.x0 = p->x0;
   P.y0 = p->y0;
-  // init_grid, src/geometry_2d.f90:240-300
-  P.dx = p->cell_size;
-  P.dy = p->cell_size;
+  // init_grid, src/geometry_2d.f90:250-266: a direction of one cell has
+  // spacing 1
+  P.dx = (P.nx > 1) ? p->cell_size : 1.0;
+  P.dy = (P.ny > 1) ? p->cell_size : 1.0;
   P.dx2 = P.dx / 2.0;
   P.dy2 = P.dy / 2.0;
   P.one_by_dx = 1.0 / P.dx;
@@ -1847,7 +1852,7 @@ __global__ void __launch_bounds__(FLUX_THREADS)
       int jj = e % (TX + 1), kk = e / (TX + 1);
       int ja = j0 + jj - 1, ka = k0 + kk, ia_x = jj - 1 + HALO, ia_y = kk + HALO;
       S.ax[kk][jj] = 0.0;
-      if (ka >= ny || ja + 1 > nx) continue;
+      if (ka >= ny || ja + 1 > nx || nx == 1) continue;
       bool a_in = ja >= 0, b_in = ja + 1 < nx;
       bool sa = a_in && (S.tile.info[ia_y][ia_x] & 128);
       bool sb = b_in && (S.tile.info[ia_y][ia_x + 1] & 128);
@@ -1861,7 +1866,7 @@ __global__ void __launch_bounds__(FLUX_THREADS)
       int jj = e2 % TX, kk = e2 / TX;
       int ja = j0 + jj, ka = k0 + kk - 1, ia_x = jj + HALO, ia_y = kk - 1 + HALO;
       S.ay[kk][jj] = 0.0;
-      if (ja >= nx || ka + 1 > ny) continue;
+      if (ja >= nx || ka + 1 > ny || ny == 1) continue;
       bool a_in = ka >= 0, b_in = ka + 1 < ny;
       bool sa = a_in && (S.tile.info[ia_y][ia_x] & 128);
       bool sb = b_in && (S.tile.info[ia_y + 1][ia_x] & 128);

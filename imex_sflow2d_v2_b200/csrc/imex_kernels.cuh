@@ -594,7 +594,12 @@ __global__ void __launch_bounds__(FLUX_THREADS, flux_min_blocks<NS>())
     }
     double& a_slot = (dir == 1) ? S.A.ax[kk][jj] : S.A.ay[kk][jj];
     const bool exists = (dir == 1) ? !(ka >= ny || ja + 1 > nx) : !(ja >= nx || ka + 1 > ny);
-    if (!exists) { a_slot = 0.0; continue; }
+    // a direction of one cell has no fluxes and no speeds: the reference
+    // skips its speeds, fluxes and divergence term (src/solver_2d.f90:
+    // 2667-2681, 3946-4001), and its zero-initialised speed arrays give no
+    // CFL limit there
+    const bool flat = (dir == 1) ? nx == 1 : ny == 1;
+    if (!exists || flat) { a_slot = 0.0; continue; }
     if (dir == 1) {
       a_in = ja >= 0;
       b_in = ja + 1 < nx;
@@ -645,7 +650,7 @@ __global__ void __launch_bounds__(FLUX_THREADS, flux_min_blocks<NS>())
 #pragma unroll
     for (int i = 0; i < NV; ++i) {
       double d = 0.0;
-      d = d + (S.H.Hx[i][kk][jj + 1] - S.H.Hx[i][kk][jj]) * P.one_by_dx;
+      if (nx > 1) d = d + (S.H.Hx[i][kk][jj + 1] - S.H.Hx[i][kk][jj]) * P.one_by_dx;
       dX[i] = d;
     }
     const double max_a = fmax_f(S.A.ax[kk][jj], S.A.ax[kk][jj + 1]);
@@ -679,7 +684,7 @@ __global__ void __launch_bounds__(FLUX_THREADS, flux_min_blocks<NS>())
 #pragma unroll
     for (int i = 0; i < NV; ++i) {
       double d = dX[i];
-      d = d + (S.H.Hy[i][kk + 1][jj] - S.H.Hy[i][kk][jj]) * P.one_by_dy;
+      if (ny > 1) d = d + (S.H.Hy[i][kk + 1][jj] - S.H.Hy[i][kk][jj]) * P.one_by_dy;
       X[c + (size_t)i * P.plane] = d - ex[i];
     }
     const double max_a = fmax_f(S.A.ay[kk][jj], S.A.ay[kk + 1][jj]);

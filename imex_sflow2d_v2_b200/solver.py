@@ -19,7 +19,10 @@ from .abi import (IMEX_OK, STATUS_NAMES, ImexOutputSpec, ImexParams, ImexPostDia
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libimexgpu.so")
-_LIB = None
+# fast mode: the same sources built with contracted multiply-adds; results
+# differ from the exact mode (and the oracle) by rounding only
+LIB_FAST_PATH = os.path.join(_HERE, "libimexgpu_fast.so")
+_LIBS = {}
 
 
 class ImexError(RuntimeError):
@@ -29,13 +32,15 @@ class ImexError(RuntimeError):
         super().__init__("%s failed: %s %s" % (where, name, detail))
 
 
-def load_library(path=LIB_PATH):
-    """Load libimexgpu.so (built by ``python -m imex_sflow2d_v2_b200.build``)."""
-    global _LIB
-    if _LIB is not None:
-        return _LIB
+def load_library(path=None, fast=False):
+    """Load libimexgpu.so, or libimexgpu_fast.so with `fast` (built by
+    ``python -m imex_sflow2d_v2_b200.build``)."""
+    if path is None:
+        path = LIB_FAST_PATH if fast else LIB_PATH
+    if path in _LIBS:
+        return _LIBS[path]
     if not os.path.exists(path):
-        raise RuntimeError("libimexgpu.so not found at %s: build it with "
+        raise RuntimeError("%s not found: build it with "
                            "`python -m imex_sflow2d_v2_b200.build`" % path)
     L = C.CDLL(path)
     vp = C.c_void_p
@@ -113,7 +118,7 @@ def load_library(path=LIB_PATH):
         f = getattr(L, name)
         f.argtypes = args
         f.restype = res
-    _LIB = L
+    _LIBS[path] = L
     return L
 
 
@@ -132,10 +137,12 @@ def measure_fp64_peak(device=-1):
 
 
 class ImexSolver:
-    """One device context holding the state of one run."""
+    """One device context holding the state of one run.  `fast` selects the
+    library built with contracted multiply-adds (results equal the exact
+    mode's to rounding, not bit for bit)."""
 
-    def __init__(self, params, static_arrays, device=-1, _handle=None):
-        self.lib = load_library()
+    def __init__(self, params, static_arrays, device=-1, _handle=None, fast=False):
+        self.lib = load_library(fast=fast)
         self.params = params
         self.nx, self.ny, self.ns = params.nx, params.ny, params.n_solid
         self.nv = 4 + self.ns

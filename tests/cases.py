@@ -200,8 +200,18 @@ def edge_variants():
     # all dry: only the border rows are solved
     p, st, q = dambreak(rheology=1)
     out["all_dry"] = (p, st, np.zeros_like(q))
-    # smallest grid the path accepts
+    # a 3x5 grid; one-row and one-column grids (no fluxes, divergence or
+    # CFL limit across the one-cell direction, whose spacing is 1)
     out["tiny_3x5"] = configs.dambreak(nx=3, ny=5, dx=0.25, rheology=1, x_split=0.4)
+    out["one_row_60x1"] = configs.dambreak(nx=60, ny=1, dx=0.25, rheology=1, x_split=7.0)
+    p, st, q = configs.dambreak(nx=1, ny=60, dx=0.25, rheology=6)
+    _, _, _, yc = configs.grid(p)
+    qp = np.zeros((7, 1, 60))
+    qp[0, 0] = np.where(yc < 7.0, 1.0, 0.1)
+    qp[3] = 300.0
+    qp[4] = 0.01 * qp[0]
+    out["one_column_1x60"] = (p, st, configs.qp_to_qc_grid(p, qp))
+    out["single_cell_1x1"] = configs.dambreak(nx=1, ny=1, dx=0.25, rheology=1)
     return out
 
 
@@ -218,3 +228,64 @@ def fractal_topo(n=48):
     st.update(geo)
     st.update(configs.slope_correction_planes(geo))
     return p, st, q
+
+
+def _one_row_case(name):
+    """The reference's TESTS/TEST_BW or TESTS/TEST_BOX run (400 x 1 cells of
+    125 m; quadratic friction 1e-3, settling and entrainment, one solid
+    class of 2000 kg/m^3, minmod, theta 1.3, CFL 0.24, MAX_DT 0.2, DT0 1e-4)
+    from the committed fixture (restart and DEM sampled at the cell
+    centres).  TEST_BW: a 400 m deep current enters through a Dirichlet west
+    boundary at 25 m/s over a ramp; TEST_BOX: a 9-cell box released on a
+    flat bed.  The east boundary is zero-gradient.  Returns (p, st, q,
+    t_end)."""
+    import os
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "bw_box_inputs.npz"))
+    nx, ny, cs = int(d["nx"]), int(d["ny"]), float(d["cell_size"])
+    p = configs.default_params(nx, ny, 1, cs, x0=float(d["x0"]), y0=float(d["y0"]))
+    p.rho_s[0] = 2000.0
+    p.diam_s[0] = 1e-3 if name == "bw" else 1e-4
+    p.sp_heat_s[0] = 1617.0
+    p.settling_flag = 1
+    p.entrainment_flag = 1
+    p.erosion_coeff = 0.0
+    p.erodible_porosity = 0.0
+    p.erodible_fract[0] = 1.0
+    p.T_erodible = 300.0
+    p.rho_c_sub = p.pres / (p.sp_gas_const_a * p.T_erodible)
+    p.coeff_porosity = 0.0
+    p.rheology_flag = 1
+    p.rheology_model = 6
+    p.friction_factor = 1.0e-3
+    p.cfl = 0.23999999463558197
+    p.max_dt = 0.2
+    p.theta = 1.3
+    # boundary variables: h, hu, hv, T, h*alpha_s (src/inpout_2d.f90:2304-2306,2876,2895)
+    if name == "bw":
+        for i, v in enumerate((400.0, 10000.0, 0.0, 900.0, 0.1)):
+            configs.set_bc(p, "W", i, 0, v)
+    else:
+        for i in range(5):
+            configs.set_bc(p, "W", i, 1, 0.0)
+        configs.set_bc(p, "W", 2, 0, 0.0)
+    for i in range(5):
+        configs.set_bc(p, "E", i, 1, 0.0)
+    configs.set_bc(p, "E", 2, 0, 0.0)
+    for side in "SN":              # not read for a one-row grid; never used
+        for i in range(5):
+            configs.set_bc(p, side, i, 1, 0.0)
+    B = np.asfortranarray(d[name + "_B_cent"])
+    st = {"B_cent": B, "solve_mask_time": np.zeros((nx, ny)),
+          "erodible": np.zeros((1, nx, ny)), "deposit": np.zeros((nx, ny, 1)),
+          "erosion": np.zeros((nx, ny, 1))}
+    st.update(configs.topography_geom(B, cs, 1.0))
+    t_end = 400.0 if name == "bw" else 200.0
+    return p, st, np.asfortranarray(d[name + "_q"]), t_end
+
+
+def test_bw():
+    return _one_row_case("bw")
+
+
+def test_box():
+    return _one_row_case("box")

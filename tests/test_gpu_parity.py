@@ -193,3 +193,41 @@ def test_moving_bed_topography_update_bitexact():
         np.testing.assert_array_equal(a, b)
     B0 = np.asarray(st["B_cent"])
     assert not np.array_equal(o.get_exchange()[3], B0)   # the bed did move
+
+
+@pytest.mark.parametrize("name", ["bw", "box"])
+def test_reference_one_row_runs_bitexact(name):
+    """The reference's 400 x 1 test runs (TESTS/TEST_BW, TESTS/TEST_BOX) to
+    their T_END through the driver loop with its dt clipping (DT0 = 1e-4),
+    on one row of cells: no y fluxes, no y divergence term, dy = 1.
+    TEST_BW's hot inflow (900 K, solid volume fraction 2.5e-4) is lighter
+    than the ambient air, so the reference's lift-off rule empties the
+    first cell after every step; TEST_BOX releases a 9-cell box on a flat
+    bed."""
+    from imex_sflow2d_v2_b200.solver import ImexSolver
+    from oracle import Oracle
+    p, st, q, t_end = getattr(cases, "test_" + name)()
+    o = Oracle(p, st, threads=8)
+    g = ImexSolver(p, st)
+    for x in (o, g):
+        x.set_state(q, 0.0)
+        x.set_clock(0.0, 1e-4, t_end=t_end, t_output=t_end)
+    step, t = 0, 0.0
+    while t < t_end:
+        eo, to = o.advance(1)
+        eg, tg = g.advance(1)
+        step += 1
+        assert tg == to, step
+        t = to
+        so, sg = o.stats(), g.stats()
+        assert (so.error_mask, so.first_error_code, so.first_error_j, so.first_error_k) == \
+            (sg.error_mask, sg.first_error_code, sg.first_error_j, sg.first_error_k), step
+        if step % 50 == 0 or t >= t_end:
+            assert np.array_equal(o.get_state(), g.get_state()), step
+            for a, b in zip(o.get_masks(), g.get_masks()):
+                assert np.array_equal(a, b), step
+            for a, b in zip(o.get_exchange(), g.get_exchange()):
+                assert np.array_equal(a, b), step
+        assert step < 5000
+    assert t == t_end and step >= 200
+    assert o.stale_wet_reads() == 0
