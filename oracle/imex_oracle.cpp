@@ -308,6 +308,8 @@ struct OracleCtx {
                                 double* dep, double& cpe, double& cpl, double* eqns,
                                 double& topo, uint32_t& err) const;
   void eval_source_bdry(double time, double vx, double vy, double* sb) const;
+  void kt_face(const double* qLf, const double* qpLf, const double* qRf, const double* qpRf,
+               double aN, double aP, double gcf, int dir, double* H) const;
   static double minmod(double a, double b);
   static double maxmod(double a, double b);
   double limit(const double* v, const double* z, int lim) const;
@@ -1390,39 +1392,57 @@ void OracleCtx::eval_speeds() {
   }
 }
 
-// src/solver_2d.f90:2832-3000 + average_KT :3017-3047
+// One interface of eval_flux_KT (src/solver_2d.f90:2862-2923 for x, dir 1;
+// :2932-2990 for y, dir 2) + average_KT (:3017-3047): the physical fluxes of
+// both face states, the KT combination, the solid-flux cap (x: .GE., y: .GT.)
+// and the zero-velocity rule (x: qp(2) of both faces; y: q(3) of both faces).
+void OracleCtx::kt_face(const double* qLf, const double* qpLf, const double* qRf,
+                        const double* qpRf, double aN, double aP, double gcf, int dir,
+                        double* H) const {
+  double fluxL[MAXV], fluxR[MAXV], avg[MAXV];
+  eval_fluxes(qLf, qpLf, gcf, dir, fluxL);
+  eval_fluxes(qRf, qpRf, gcf, dir, fluxR);
+  for (int i = 0; i < nv; ++i)
+    avg[i] = (aN == aP) ? 0.0 : (aP * fluxL[i] - aN * fluxR[i]) / (aP - aN);
+  for (int i = 0; i < nv; ++i) {
+    if (aN == aP)
+      H[i] = 0.0;
+    else
+      H[i] = avg[i] + (aP * aN) / (aP - aN) * (qRf[i] - qLf[i]);
+  }
+  double s = 0.0;
+  for (int i = 0; i < ns; ++i) s += H[4 + i];
+  if (dir == 1) {
+    if (s / H[0] >= 1.0) {
+      double r = 0.0;
+      for (int i = 0; i < ns; ++i) r += H[4 + i] / H[0];
+      for (int i = 0; i < ns; ++i) H[4 + i] = H[4 + i] / r;
+    }
+    if (qpLf[1] == 0.0 && qpRf[1] == 0.0) {
+      H[0] = 0.0;
+      for (int i = 3; i < nv; ++i) H[i] = 0.0;
+    }
+  } else {
+    if (s / H[0] > 1.0) {
+      double r = s / H[0];
+      for (int i = 0; i < ns; ++i) H[4 + i] = H[4 + i] / r;
+    }
+    if (qLf[2] == 0.0 && qRf[2] == 0.0) {
+      H[0] = 0.0;
+      for (int i = 3; i < nv; ++i) H[i] = 0.0;
+    }
+  }
+}
+
+// src/solver_2d.f90:2832-3000
 void OracleCtx::eval_flux_KT() {
   if (nx > 1) {
 #pragma omp parallel for schedule(static)
     for (int64_t l = 0; l < solve_interfaces_x; ++l) {
       int j = j_stag_x[l], k = k_stag_x[l];
       size_t f = sx2(j, k);
-      double fluxL[MAXV], fluxR[MAXV], avg[MAXV];
-      eval_fluxes(FX(qL, nv, j, k), FX(qpL, np, j, k), gc_sx[f], 1, fluxL);
-      eval_fluxes(FX(qR, nv, j, k), FX(qpR, np, j, k), gc_sx[f], 1, fluxR);
-      double aN = axNeg[f], aP = axPos[f];
-      double* H = FX(Hx, nv, j, k);
-      for (int i = 0; i < nv; ++i)
-        avg[i] = (aN == aP) ? 0.0 : (aP * fluxL[i] - aN * fluxR[i]) / (aP - aN);
-      const double* qLf = FX(qL, nv, j, k);
-      const double* qRf = FX(qR, nv, j, k);
-      for (int i = 0; i < nv; ++i) {
-        if (aN == aP)
-          H[i] = 0.0;
-        else
-          H[i] = avg[i] + (aP * aN) / (aP - aN) * (qRf[i] - qLf[i]);
-      }
-      double s = 0.0;
-      for (int i = 0; i < ns; ++i) s += H[4 + i];
-      if (s / H[0] >= 1.0) {
-        double r = 0.0;
-        for (int i = 0; i < ns; ++i) r += H[4 + i] / H[0];
-        for (int i = 0; i < ns; ++i) H[4 + i] = H[4 + i] / r;
-      }
-      if (FX(qpL, np, j, k)[1] == 0.0 && FX(qpR, np, j, k)[1] == 0.0) {
-        H[0] = 0.0;
-        for (int i = 3; i < nv; ++i) H[i] = 0.0;
-      }
+      kt_face(FX(qL, nv, j, k), FX(qpL, np, j, k), FX(qR, nv, j, k), FX(qpR, np, j, k),
+              axNeg[f], axPos[f], gc_sx[f], 1, FX(Hx, nv, j, k));
     }
   }
   if (ny > 1) {
@@ -1430,31 +1450,8 @@ void OracleCtx::eval_flux_KT() {
     for (int64_t l = 0; l < solve_interfaces_y; ++l) {
       int j = j_stag_y[l], k = k_stag_y[l];
       size_t f = sy2(j, k);
-      double fluxB[MAXV], fluxT[MAXV], avg[MAXV];
-      eval_fluxes(FY(qB, nv, j, k), FY(qpB, np, j, k), gc_sy[f], 2, fluxB);
-      eval_fluxes(FY(qT, nv, j, k), FY(qpT, np, j, k), gc_sy[f], 2, fluxT);
-      double aN = ayNeg[f], aP = ayPos[f];
-      double* H = FY(Hy, nv, j, k);
-      for (int i = 0; i < nv; ++i)
-        avg[i] = (aN == aP) ? 0.0 : (aP * fluxB[i] - aN * fluxT[i]) / (aP - aN);
-      const double* qBf = FY(qB, nv, j, k);
-      const double* qTf = FY(qT, nv, j, k);
-      for (int i = 0; i < nv; ++i) {
-        if (aN == aP)
-          H[i] = 0.0;
-        else
-          H[i] = avg[i] + (aP * aN) / (aP - aN) * (qTf[i] - qBf[i]);
-      }
-      double s = 0.0;
-      for (int i = 0; i < ns; ++i) s += H[4 + i];
-      if (s / H[0] > 1.0) {
-        double r = s / H[0];
-        for (int i = 0; i < ns; ++i) H[4 + i] = H[4 + i] / r;
-      }
-      if (qBf[2] == 0.0 && qTf[2] == 0.0) {
-        H[0] = 0.0;
-        for (int i = 3; i < nv; ++i) H[i] = 0.0;
-      }
+      kt_face(FY(qB, nv, j, k), FY(qpB, np, j, k), FY(qT, nv, j, k), FY(qpT, np, j, k),
+              ayNeg[f], ayPos[f], gc_sy[f], 2, FY(Hy, nv, j, k));
     }
   }
 }
@@ -2568,6 +2565,45 @@ void oracle_implicit_terms(OracleCtx* o, const double* q_re, const double* q_im,
   for (int i = 0; i < o->nv; ++i) {
     nh_re[i] = nh[i].re;
     if (nh_im) nh_im[i] = nh[i].im;
+  }
+}
+
+void oracle_mixt_var(OracleCtx* o, const double* qp, double* out) {
+  double Ri, rho_m, rho_c, red_grav, spc, spm;
+  o->mixt_var(qp, Ri, rho_m, rho_c, red_grav, false, spc, spm);
+  out[0] = Ri;
+  out[1] = rho_m;
+  out[2] = rho_c;
+  out[3] = red_grav;
+}
+
+void oracle_local_speeds(OracleCtx* o, const double* qp, double gcf, int dir, double* out) {
+  if (dir == 1)
+    o->eval_local_speeds_x(qp, gcf, out[0], out[1]);
+  else
+    o->eval_local_speeds_y(qp, gcf, out[0], out[1]);
+}
+
+void oracle_eval_fluxes(OracleCtx* o, const double* qc, const double* qp, double gcf, int dir,
+                        double* flux) {
+  o->eval_fluxes(qc, qp, gcf, dir, flux);
+}
+
+void oracle_kt_interface(OracleCtx* o, const double* qcL, const double* qpL, const double* qcR,
+                         const double* qpR, double gcf, int dir, double* H, double* speeds) {
+  double lmin, lmax, rmin, rmax;
+  if (dir == 1) {
+    o->eval_local_speeds_x(qpL, gcf, lmin, lmax);
+    o->eval_local_speeds_x(qpR, gcf, rmin, rmax);
+  } else {
+    o->eval_local_speeds_y(qpL, gcf, lmin, lmax);
+    o->eval_local_speeds_y(qpR, gcf, rmin, rmax);
+  }
+  const double aN = fmin_f(fmin_f(lmin, rmin), 0.0), aP = fmax_f(fmax_f(lmax, rmax), 0.0);
+  o->kt_face(qcL, qpL, qcR, qpR, aN, aP, gcf, dir, H);
+  if (speeds) {
+    speeds[0] = aN;
+    speeds[1] = aP;
   }
 }
 

@@ -71,6 +71,16 @@ void oracle_implicit_terms(OracleCtx* o, const double* q_re, const double* q_im,
 int oracle_solve_rk_step(OracleCtx* o, double* qj, const double* qj_old,
                          const double* rj_not_impl, double bprime_x,
                          double bprime_y, double dt, double a_diag);
+/* mixt_var (Ri, rho_m, rho_c, red_grav) of one physical state */
+void oracle_mixt_var(OracleCtx* o, const double* qp, double* out /* 4 */);
+/* eval_local_speeds_x (dir 1) / _y (dir 2): out = (vel_min, vel_max) */
+void oracle_local_speeds(OracleCtx* o, const double* qp, double gcf, int dir, double* out);
+void oracle_eval_fluxes(OracleCtx* o, const double* qc, const double* qp, double gcf, int dir,
+                        double* flux);
+/* one KT interface from its two face states (speeds, fluxes, average_KT,
+ * solid-flux cap, zero-velocity rule); speeds (may be NULL) = (a-, a+) */
+void oracle_kt_interface(OracleCtx* o, const double* qcL, const double* qpL, const double* qcR,
+                         const double* qpR, double gcf, int dir, double* H, double* speeds);
 double oracle_ipow(double x, double y);
 double oracle_limit(double v1, double v2, double v3, double z1, double z2,
                     double z3, int limiter, double theta);

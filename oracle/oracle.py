@@ -80,6 +80,10 @@ def lib(target=CHECKER):
         L.oracle_qc_to_qp.argtypes = [vp, dp, dp]
         L.oracle_qp_to_qc.argtypes = [vp, dp, dp]
         L.oracle_implicit_terms.argtypes = [vp, dp, dp, dp, dp]
+        L.oracle_mixt_var.argtypes = [vp, dp, dp]
+        L.oracle_local_speeds.argtypes = [vp, dp, C.c_double, C.c_int, dp]
+        L.oracle_eval_fluxes.argtypes = [vp, dp, dp, C.c_double, C.c_int, dp]
+        L.oracle_kt_interface.argtypes = [vp, dp, dp, dp, dp, C.c_double, C.c_int, dp, dp]
         L.oracle_solve_rk_step.restype = C.c_int
         L.oracle_solve_rk_step.argtypes = [vp, dp, dp, dp, C.c_double, C.c_double,
                                            C.c_double, C.c_double]
@@ -259,6 +263,35 @@ class Oracle:
         out = np.zeros(self.nv)
         self._L.oracle_qp_to_qc(self._h, _p(qp), _p(out))
         return out
+
+    def mixt_var(self, qp):
+        """(Ri, rho_m, rho_c, red_grav) of one physical state."""
+        qp = np.ascontiguousarray(qp, dtype=np.float64)
+        out = np.zeros(4)
+        self._L.oracle_mixt_var(self._h, _p(qp), _p(out))
+        return out
+
+    def local_speeds(self, qp, gcf, d):
+        qp = np.ascontiguousarray(qp, dtype=np.float64)
+        out = np.zeros(2)
+        self._L.oracle_local_speeds(self._h, _p(qp), float(gcf), int(d), _p(out))
+        return out
+
+    def eval_fluxes(self, qc, qp, gcf, d):
+        qc = np.ascontiguousarray(qc, dtype=np.float64)
+        qp = np.ascontiguousarray(qp, dtype=np.float64)
+        out = np.zeros(self.nv)
+        self._L.oracle_eval_fluxes(self._h, _p(qc), _p(qp), float(gcf), int(d), _p(out))
+        return out
+
+    def kt_interface(self, qcL, qpL, qcR, qpR, gcf, d):
+        """(H, (a-, a+)) of one interface from its two face states."""
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (qcL, qpL, qcR, qpR)]
+        H = np.zeros(self.nv)
+        sp = np.zeros(2)
+        self._L.oracle_kt_interface(self._h, *[_p(x) for x in a], float(gcf), int(d), _p(H),
+                                    _p(sp))
+        return H, sp
 
     def implicit_terms(self, q_re, q_im=None):
         q_re = np.ascontiguousarray(q_re, dtype=np.float64)
