@@ -82,6 +82,15 @@ def transmissive_bcs(p):
             set_bc(p, side, i, 2)
 
 
+def zero_gradient_bcs(p):
+    """Every variable zero-gradient Neumann (flag 1, value 0) on every side --
+    the boundary set of the reference's ensemble example
+    (EXAMPLES/EXAMPLE_ENSEMBLE_ETNA/templatedir/IMEX_SfloW2D.inp:42-87)."""
+    for side in "WESN":
+        for i in range(4 + p.n_solid):
+            set_bc(p, side, i, 1, 0.0)
+
+
 def grid(p):
     """x_stag, x_comp, y_stag, y_comp as in init_grid (geometry_2d.f90:292-314)."""
     nx, ny = p.nx, p.ny
@@ -480,7 +489,8 @@ def fractal_inlet(n=4096, dx=10.0, hurst=0.8, relief=800.0, slope_deg=15.0,
 
 def ensemble_members(n_members=256, side_min=256, side_max=1024, dx=2.0, seed=20261204,
                      bump_h=(5.0, 50.0), bump_sigma=(50.0, 300.0), mfr=(1.0e6, 1.0e8),
-                     T_source=(600.0, 1200.0), diam=(1.0e-5, 1.0e-3), r_source=20.0):
+                     T_source=(600.0, 1200.0), diam=(1.0e-5, 1.0e-3), r_source=20.0,
+                     bcs="ensemble"):
     """Batched-ensemble workload (fourth workload): members on their own
     square grids of 2 m cells, side uniform in [side_min, side_max]; a
     Gaussian bump of uniform random height and sigma; a radial inlet of
@@ -488,8 +498,12 @@ def ensemble_members(n_members=256, side_min=256, side_max=1024, dx=2.0, seed=20
     class of log-uniform diameter (95% solid by mass, Voellmy friction as in
     the radial-current workload).  The sampling follows the reference's
     ensemble example (EXAMPLES/EXAMPLE_ENSEMBLE_ETNA/create_ensemble.py:35-55:
-    log-uniform and uniform 1-D sampling).  Returns a list of
-    (params, static, q, sample) with `sample` the drawn values."""
+    log-uniform and uniform 1-D sampling), and so do the boundaries: every
+    variable zero-gradient (bcs="ensemble"); bcs="dambreak" keeps the
+    radial-current workload's TEST_DAMBREAK set (h extrapolated by the
+    one-sided slope), under which thick currents that reach the border
+    break down.  Returns a list of (params, static, q, sample) with `sample`
+    the drawn values."""
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(n_members):
@@ -503,5 +517,7 @@ def ensemble_members(n_members=256, side_min=256, side_max=1024, dx=2.0, seed=20
         p, st, q = radial_current(nx=side, ny=side, dx=dx, bump_h=s["bump_h"],
                                   bump_sigma=s["bump_sigma"], r_source=r_source, mfr=s["mfr"],
                                   T_source=s["T_source"], xs=(0.95,), diam=(s["diam"],))
+        if bcs == "ensemble":
+            zero_gradient_bcs(p)
         out.append((p, st, q, s))
     return out

@@ -132,15 +132,19 @@ def test_repeat_runs_are_bit_identical():
 
 
 def test_ensemble_member_breakdown_bitexact():
-    """A member of the ensemble workload (341^2, 7.1e6 kg/s) whose current
-    reaches the west boundary: the reference's checks fire from step ~407
-    (T < 273 K, then solid sum, negative h), dt collapses and q turns NaN at
-    step ~466.  The CUDA path follows the oracle through all of it, step for
-    step (NaNs compared as equal, whatever their payload)."""
+    """A member of the ensemble workload (341^2, 7.1e6 kg/s, a 660 m thick
+    inlet current) under the TEST_DAMBREAK boundary set, whose current
+    reaches the west boundary: there h is extrapolated by the one-sided
+    slope while hu is zero-gradient, so the west face of cell (1,167) gets
+    h = (3*3.396 - 10.065)/2 = 0.06 m with hu = -575 m^2/s, a face velocity
+    of -9350 m/s.  The reference's checks fire from step 407 (T < 273 K,
+    then solid sum, negative h), dt collapses and q turns NaN at step ~466.
+    The CUDA path follows the oracle through all of it, step for step (NaNs
+    compared as equal, whatever their payload)."""
     from imex_sflow2d_v2_b200 import configs
     from imex_sflow2d_v2_b200.solver import ImexSolver
     from oracle import Oracle
-    p, st, q, s = configs.ensemble_members(n_members=13)[12]
+    p, st, q, s = configs.ensemble_members(n_members=13, bcs="dambreak")[12]
     o = Oracle(p, st, threads=8)
     g = ImexSolver(p, st)
     for x in (o, g):
