@@ -396,7 +396,11 @@ def radial_current(nx=1024, ny=1024, dx=2.0, bump_h=20.0, bump_sigma=200.0,
     workload: 1024^2 cells of 2 m, circular inlet r=20 m at 5e6 kg/s, T=900 K,
     two solid classes split 0.6/0.4 of the solid mass, Voellmy mu=0.1 xi=500).
     The inlet carries 95% solid by mass (the split of the two classes is
-    0.6/0.4); VEL_SOURCE = 10 m/s."""
+    0.6/0.4); VEL_SOURCE = 10 m/s.  Every boundary variable is zero-gradient,
+    the boundary set of the reference's ensemble example for radial
+    currents (zero_gradient_bcs); under the dam-break set (h extrapolated by
+    its one-sided slope) the 510 m thick current breaks down where it
+    reaches the border."""
     ns = len(xs)
     p = default_params(nx, ny, ns, dx)
     for i in range(ns):
@@ -407,7 +411,7 @@ def radial_current(nx=1024, ny=1024, dx=2.0, bump_h=20.0, bump_sigma=200.0,
     p.rheology_model = 1
     p.mu, p.xi = mu, xi
     p.max_dt = 1.0
-    transmissive_bcs(p)
+    zero_gradient_bcs(p)
     _, x_comp, _, y_comp = grid(p)
     xs0 = x_comp[nx // 2]
     ys0 = y_comp[ny // 2]
@@ -517,7 +521,7 @@ def ensemble_members(n_members=256, side_min=256, side_max=1024, dx=2.0, seed=20
         p, st, q = radial_current(nx=side, ny=side, dx=dx, bump_h=s["bump_h"],
                                   bump_sigma=s["bump_sigma"], r_source=r_source, mfr=s["mfr"],
                                   T_source=s["T_source"], xs=(0.95,), diam=(s["diam"],))
-        if bcs == "ensemble":
-            zero_gradient_bcs(p)
+        if bcs == "dambreak":
+            transmissive_bcs(p)
         out.append((p, st, q, s))
     return out
