@@ -18,19 +18,39 @@
 // element (j,k) (0-based) at k*pitch + j.
 #pragma once
 
+#include <type_traits>
+
 #include "imex_device.cuh"
 #include "imex_mlp.cuh"
 
 namespace imex {
 
-constexpr int TX = 32;
-constexpr int TY = 8;
 constexpr int HALO = 2;
-constexpr int SW = TX + 2 * HALO;  // shared tile width
-constexpr int SH = TY + 2 * HALO;  // shared tile height
-constexpr int FLUX_THREADS = 288;
-constexpr int NXI = (TX + 1) * TY;  // x-interfaces per tile
-constexpr int NYI = TX * (TY + 1);  // y-interfaces per tile
+
+// A tile of TXv x TYv cells: its shared-memory extent with the 2-cell halo,
+// its interface counts and the threads of a flux block (one per cell, plus
+// one warp, so that every cell keeps its own thread between the x and y
+// phases of k_flux).
+template <int TXv, int TYv>
+struct TileShape {
+  static constexpr int TX = TXv, TY = TYv;
+  static constexpr int SW = TX + 2 * HALO;    // shared tile width
+  static constexpr int SH = TY + 2 * HALO;    // shared tile height
+  static constexpr int NXI = (TX + 1) * TY;   // x-interfaces per tile
+  static constexpr int NYI = TX * (TY + 1);   // y-interfaces per tile
+  static constexpr int THREADS = TX * TY + 32;
+};
+using Shape32x8 = TileShape<32, 8>;    // the single-grid path's tiles
+using Shape16x16 = TileShape<16, 16>;
+using Shape32x4 = TileShape<32, 4>;
+
+constexpr int TX = Shape32x8::TX;
+constexpr int TY = Shape32x8::TY;
+constexpr int SW = Shape32x8::SW;
+constexpr int SH = Shape32x8::SH;
+constexpr int FLUX_THREADS = Shape32x8::THREADS;
+constexpr int NXI = Shape32x8::NXI;
+constexpr int NYI = Shape32x8::NYI;
 
 // Minimum resident blocks per SM asked of ptxas for the flux and per-cell
 // kernels (their register budget); tuning knobs, set with -D at build time.
@@ -85,20 +105,21 @@ __device__ const RingCell* find_ring(const RingCell* ring, int n, long long idx)
 }
 
 // ================================================================= k_mask
-// check_solve(.FALSE.) for n_RK = 2.
-__global__ void __launch_bounds__(256) k_mask(const __grid_constant__ DevParams Pp, const double* __restrict__ q1,
-                                              const double* __restrict__ release_time,
-                                              const uint8_t* __restrict__ cellinfo,
-                                              const DevClock* clk, uint8_t* __restrict__ mask,
-                                              DevClock* clkw, int solve_all) {
-  const DevParams& P = Pp;
-  __shared__ uint8_t s0[SH][SW];
-  __shared__ uint8_t s1[SH][SW];
-  const int j0 = blockIdx.x * TX, k0 = blockIdx.y * TY;
-  const double t = clk->t;
+// check_solve(.FALSE.) for n_RK = 2 on the tile whose first cell is
+// (j0, k0): the wet/source seed of the tile and a 2-cell halo, two 4-point
+// dilations, the border rows and the inlet-interior removal.  Returns, to
+// every thread of the block, whether any cell of the tile is solved.
+template <class TS>
+__device__ __forceinline__ bool mask_tile(const DevParams& P, const double* __restrict__ q1,
+                                          const double* __restrict__ release_time,
+                                          const uint8_t* __restrict__ cellinfo, double t,
+                                          uint8_t* __restrict__ mask, DevClock* clkw,
+                                          int solve_all, int j0, int k0,
+                                          uint8_t (*s0)[TS::SW], uint8_t (*s1)[TS::SW]) {
+  constexpr int SWt = TS::SW, SHt = TS::SH, TXt = TS::TX, TYt = TS::TY;
   const int nx = P.nx, ny = P.ny;
-  for (int e = threadIdx.x; e < SW * SH; e += blockDim.x) {
-    int lx = e % SW, ly = e / SW;
+  for (int e = threadIdx.x; e < SWt * SHt; e += blockDim.x) {
+    int lx = e % SWt, ly = e / SWt;
     int j = j0 + lx - HALO, k = k0 + ly - HALO;
     uint8_t m = 0;
     if (j >= 0 && j < nx && k >= 0 && k < ny) {
@@ -116,19 +137,19 @@ __global__ void __launch_bounds__(256) k_mask(const __grid_constant__ DevParams 
   }
   __syncthreads();
   // first dilation on the tile plus a 1-cell ring
-  for (int e = threadIdx.x; e < SW * SH; e += blockDim.x) {
-    int lx = e % SW, ly = e / SW;
+  for (int e = threadIdx.x; e < SWt * SHt; e += blockDim.x) {
+    int lx = e % SWt, ly = e / SWt;
     int j = j0 + lx - HALO, k = k0 + ly - HALO;
     uint8_t m = s0[ly][lx];
-    if (lx >= 1 && lx < SW - 1 && ly >= 1 && ly < SH - 1 && j >= 1 && j < nx - 1 && k >= 1 &&
+    if (lx >= 1 && lx < SWt - 1 && ly >= 1 && ly < SHt - 1 && j >= 1 && j < nx - 1 && k >= 1 &&
         k < ny - 1)
       m = m | s0[ly][lx - 1] | s0[ly][lx + 1] | s0[ly - 1][lx] | s0[ly + 1][lx];
     s1[ly][lx] = m;
   }
   __syncthreads();
   int cnt = 0;
-  for (int e = threadIdx.x; e < TX * TY; e += blockDim.x) {
-    int lx = e % TX + HALO, ly = e / TX + HALO;
+  for (int e = threadIdx.x; e < TXt * TYt; e += blockDim.x) {
+    int lx = e % TXt + HALO, ly = e / TXt + HALO;
     int j = j0 + lx - HALO, k = k0 + ly - HALO;
     if (j >= nx || k >= ny) continue;
     uint8_t m = s1[ly][lx];
@@ -138,25 +159,38 @@ __global__ void __launch_bounds__(256) k_mask(const __grid_constant__ DevParams 
     mask[(size_t)k * P.pitch + j] = m;
     cnt += m;
   }
+  const bool any = __syncthreads_or(cnt) != 0;
   // solve-cell count
   for (int off = 16; off > 0; off >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, off);
   if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&clkw->solve_cells, (unsigned long long)cnt);
+  return any;
+}
+
+__global__ void __launch_bounds__(256) k_mask(const __grid_constant__ DevParams Pp, const double* __restrict__ q1,
+                                              const double* __restrict__ release_time,
+                                              const uint8_t* __restrict__ cellinfo,
+                                              const DevClock* clk, uint8_t* __restrict__ mask,
+                                              DevClock* clkw, int solve_all) {
+  __shared__ uint8_t s0[SH][SW];
+  __shared__ uint8_t s1[SH][SW];
+  mask_tile<Shape32x8>(Pp, q1, release_time, cellinfo, clk->t, mask, clkw, solve_all,
+                       blockIdx.x * TX, blockIdx.y * TY, s0, s1);
 }
 
 // ================================================================== faces
 // Shared tile of physical states: qps[v][ly][lx]; info_s[ly][lx] holds the
 // cellinfo bits plus bit 7 = solve mask.
-template <int NS>
+template <int NS, class TS = Shape32x8>
 struct Tile {
-  double qp[6 + NS][SH][SW];
-  uint8_t info[SH][SW];
+  double qp[6 + NS][TS::SH][TS::SW];
+  uint8_t info[TS::SH][TS::SW];
 };
 
 // Face states of one cell in one direction: W/E (dir 1) or S/N (dir 2).
 // `stage` selects the RK-stage arrays' view of never-solved inlet-interior
 // neighbours (all zero) instead of the module qp view (zero with T_ambient).
-template <int NS>
-IMEX_FLAT void cell_faces(const DevParams& P, const Tile<NS>& T, int lx, int ly, int j, int k,
+template <int NS, class TS>
+IMEX_FLAT void cell_faces(const DevParams& P, const Tile<NS, TS>& T, int lx, int ly, int j, int k,
                            int dir, bool stage, double time, const RingCell* ring,
                            double* Fm, double* Fp) {
   constexpr int NV = 4 + NS, NP = 6 + NS;
@@ -300,17 +334,17 @@ IMEX_FLAT void cell_faces(const DevParams& P, const Tile<NS>& T, int lx, int ly,
 // There the faces are qp -/+ rc_d*limit(...) for every variable, exactly the
 // operations of cell_faces.  Indexed [ly - 1][lx - 1] of the shared tile:
 // x faces use rows 2..9 and columns 1..34, y faces rows 1..10, columns 2..33.
-template <int NS>
+template <int NS, class TS = Shape32x8>
 struct SlopeTile {
-  double dq[6 + NS][TY + 2][TX + 2];
-  uint8_t ok[TY + 2][TX + 2];
+  double dq[6 + NS][TS::TY + 2][TS::TX + 2];
+  uint8_t ok[TS::TY + 2][TS::TX + 2];
 };
 
-template <int NS>
-__device__ __forceinline__ void precompute_slopes(const DevParams& P, const Tile<NS>& T,
-                                                  SlopeTile<NS>& D, int dir, int j0, int k0,
+template <int NS, class TS>
+__device__ __forceinline__ void precompute_slopes(const DevParams& P, const Tile<NS, TS>& T,
+                                                  SlopeTile<NS, TS>& D, int dir, int j0, int k0,
                                                   const uint8_t* __restrict__ mask) {
-  constexpr int NP = 6 + NS;
+  constexpr int NP = 6 + NS, TX = TS::TX, TY = TS::TY;
   const int nx = P.nx, ny = P.ny;
   const bool rad = P.radial_source_flag != 0;
   const int rw = (dir == 1) ? TX + 2 : TX, rh = (dir == 1) ? TY : TY + 2;
@@ -348,12 +382,12 @@ __device__ __forceinline__ void precompute_slopes(const DevParams& P, const Tile
   }
 }
 
-template <int NS>
-IMEX_FLAT void interface_flux(const DevParams& P, const Tile<NS>& T, int dir, int la_x,
+template <int NS, class TS>
+IMEX_FLAT void interface_flux(const DevParams& P, const Tile<NS, TS>& T, int dir, int la_x,
                                int la_y, int ja, int ka, bool a_in, bool b_in, double gcf,
                                bool stage, double time, const RingCell* ring, double* H,
                                double& amax_flux, double& aneg_out, double& apos_out,
-                               const SlopeTile<NS>* D = nullptr) {
+                               const SlopeTile<NS, TS>* D = nullptr) {
   constexpr int NV = 4 + NS, NP = 6 + NS;
   const int lb_x = (dir == 1) ? la_x + 1 : la_x, lb_y = (dir == 1) ? la_y : la_y + 1;
   const int jb = (dir == 1) ? ja + 1 : ja, kb = (dir == 1) ? ka : ka + 1;
@@ -471,32 +505,38 @@ IMEX_FLAT void interface_flux(const DevParams& P, const Tile<NS>& T, int dir, in
 // Shared memory: Tile<NS> + slopes + one direction's interface fluxes and
 // CFL speeds at a time (the x ones are reduced into each cell's registers
 // before the y phase overwrites them).
-template <int NS>
+template <int NS, class TS = Shape32x8>
 struct FluxShared {
-  Tile<NS> tile;
-  SlopeTile<NS> slopes;
+  Tile<NS, TS> tile;
+  SlopeTile<NS, TS> slopes;
   union {
-    double Hx[4 + NS][TY][TX + 1];
-    double Hy[4 + NS][TY + 1][TX];
+    double Hx[4 + NS][TS::TY][TS::TX + 1];
+    double Hy[4 + NS][TS::TY + 1][TS::TX];
   } H;
   union {
-    double ax[TY][TX + 1];
-    double ay[TY + 1][TX];
+    double ax[TS::TY][TS::TX + 1];
+    double ay[TS::TY + 1][TS::TX];
   } A;
-  double dtmin[FLUX_THREADS / 32];
+  double dtmin[TS::THREADS / 32];
 };
-static_assert(FLUX_THREADS >= TX * TY, "k_flux keeps one cell per thread between phases");
+static_assert(Shape32x8::THREADS == 288, "k_flux blocks of 288 threads for 32x8 tiles");
 
 // Blocks of k_flux per SM: 3 where three blocks' shared memory fits the SM
 // (228 KB, 1 KB reserved per block; n_s <= 3), else 2.  At n_s = 3 three
 // blocks at 72 registers measured 9.5 ms per step at 4096^2 against 10.9 at
 // two blocks of 96.
-template <int NS>
+// Other tile shapes keep the register budget of three 288-thread blocks
+// (864 threads per SM) and fit as many blocks as shared memory allows.
+template <int NS, class TS = Shape32x8>
 constexpr int flux_min_blocks() {
 #ifdef IMEX_FLUX_MINB
   return IMEX_FLUX_MINB;
 #else
-  return (3 * (sizeof(FluxShared<NS>) + 1024) <= 228 * 1024) ? 3 : 2;
+  return std::is_same<TS, Shape32x8>::value
+             ? ((3 * (sizeof(FluxShared<NS, TS>) + 1024) <= 228 * 1024) ? 3 : 2)
+             : ((864 / TS::THREADS) < (int)(228 * 1024 / (sizeof(FluxShared<NS, TS>) + 1024))
+                    ? (864 / TS::THREADS)
+                    : (int)(228 * 1024 / (sizeof(FluxShared<NS, TS>) + 1024)));
 #endif
 }
 
@@ -509,20 +549,26 @@ struct CflShared {
   double dtmin[FLUX_THREADS / 32];
 };
 
-template <int NS>
-__global__ void __launch_bounds__(FLUX_THREADS, flux_min_blocks<NS>())
-    k_flux(const __grid_constant__ DevParams Pp, const double* __restrict__ q, const uint8_t* __restrict__ mask,
-           const uint8_t* __restrict__ cellinfo, const double* __restrict__ Bx,
-           const double* __restrict__ By, const double* __restrict__ Bxx,
-           const double* __restrict__ Bxy, const double* __restrict__ Byy,
-           const double* __restrict__ gc, const double* __restrict__ dgc,
-           const double* __restrict__ gcsx, const double* __restrict__ gcsy,
-           const RingCell* __restrict__ ring, DevClock* clk, double* __restrict__ X) {
-  const DevParams& P = Pp;
+// Stage 1 and the CFL minimum on the tile whose first cell is (j0, k0).
+template <int NS, class TS>
+__device__ __forceinline__ void flux_tile(const DevParams& P, const double* __restrict__ q,
+                                          const uint8_t* __restrict__ mask,
+                                          const uint8_t* __restrict__ cellinfo,
+                                          const double* __restrict__ Bx,
+                                          const double* __restrict__ By,
+                                          const double* __restrict__ Bxx,
+                                          const double* __restrict__ Bxy,
+                                          const double* __restrict__ Byy,
+                                          const double* __restrict__ gc,
+                                          const double* __restrict__ dgc,
+                                          const double* __restrict__ gcsx,
+                                          const double* __restrict__ gcsy,
+                                          const RingCell* __restrict__ ring, DevClock* clk,
+                                          double* __restrict__ X, int j0, int k0,
+                                          FluxShared<NS, TS>& S) {
   constexpr int NV = 4 + NS, NP = 6 + NS;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  FluxShared<NS>& S = *reinterpret_cast<FluxShared<NS>*>(smem_raw);
-  const int j0 = blockIdx.x * TX, k0 = blockIdx.y * TY;
+  constexpr int TX = TS::TX, TY = TS::TY, SW = TS::SW, SH = TS::SH, NXI = TS::NXI,
+                NYI = TS::NYI;
   const int nx = P.nx, ny = P.ny;
   const double time = clk->t;
   // any solve cell in the tile?
@@ -704,6 +750,21 @@ __global__ void __launch_bounds__(FLUX_THREADS, flux_min_blocks<NS>())
     if (m >= 0.0 && m < P.max_dt)
       atomicMin(&clk->dtmin_bits, (unsigned long long)__double_as_longlong(m));
   }
+}
+
+template <int NS>
+__global__ void __launch_bounds__(FLUX_THREADS, flux_min_blocks<NS>())
+    k_flux(const __grid_constant__ DevParams Pp, const double* __restrict__ q, const uint8_t* __restrict__ mask,
+           const uint8_t* __restrict__ cellinfo, const double* __restrict__ Bx,
+           const double* __restrict__ By, const double* __restrict__ Bxx,
+           const double* __restrict__ Bxy, const double* __restrict__ Byy,
+           const double* __restrict__ gc, const double* __restrict__ dgc,
+           const double* __restrict__ gcsx, const double* __restrict__ gcsy,
+           const RingCell* __restrict__ ring, DevClock* clk, double* __restrict__ X) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FluxShared<NS>& S = *reinterpret_cast<FluxShared<NS>*>(smem_raw);
+  flux_tile<NS, Shape32x8>(Pp, q, mask, cellinfo, Bx, By, Bxx, Bxy, Byy, gc, dgc, gcsx, gcsy, ring,
+                           clk, X, blockIdx.x * TX, blockIdx.y * TY, S);
 }
 
 // =============================================================== Newton
