@@ -11,7 +11,7 @@ LIB_FAST = os.path.join(_HERE, "libimexgpu_fast.so")
 
 
 def sources():
-    return [os.path.join(CSRC, f) for f in ("imex_gpu.cu", "imex_kernels.cuh", "imex_mlp.cuh",
+    return [os.path.join(CSRC, f) for f in ("imex_gpu.cu", "imex_kernels.cuh", "imex_batch.cuh", "imex_mlp.cuh",
                                              "imex_device.cuh", "imex_setup.cuh", "imex_output.cuh",
                                              "imex_fortran_fmt.h",
                                              "ipow_tables.h")] + [

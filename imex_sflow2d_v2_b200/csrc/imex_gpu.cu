@@ -18,6 +18,7 @@
 
 #include "../../include/imex_gpu.h"
 #include "imex_kernels.cuh"
+#include "imex_batch.cuh"
 #include "imex_mlp.cuh"
 #include "imex_setup.cuh"
 #include "imex_output.cuh"
@@ -1547,6 +1548,21 @@ struct ImexEnsemble {
   std::vector<int> tried_k;
   std::vector<float> tried_ms;
   std::string last_error;
+  // batched mode: every phase one persistent kernel for all members
+  // (imex_batch.cuh); the tile shape is chosen by timing a real step with each
+  int shape = -1;                    // chosen index into kShapes (-1: not tuned yet)
+  int batch_shape = -1;              // shape the device tables are built for
+  std::vector<int> tried_shape;
+  std::vector<float> tried_shape_ms;
+  MemberDev* dM = nullptr;
+  uint32_t* tile_member = nullptr;
+  uint32_t* active = nullptr;
+  unsigned int* n_active = nullptr;
+  unsigned long long* list_off = nullptr;
+  long long n_tiles = 0;
+  size_t tile_cap = 0;               // capacity of tile_member / active
+  int64_t batch_launches = 0;        // kernels in one batched step
+  int graph_shape = -1;              // tile shape of the captured graph (-1: per-member graph)
 };
 
 namespace {
@@ -1563,6 +1579,174 @@ int ens_fail(ImexEnsemble* e, int code, const std::string& msg) {
     cudaError_t e_ = (call);                                                  \
     if (e_ != cudaSuccess) return ens_fail(ens, IMEX_ECUDA, cudaGetErrorString(e_)); \
   } while (0)
+
+void ens_drop_graph(ImexEnsemble* ens);
+
+// Tile shapes the tuner tries for the batched mode.
+struct ShapeDesc {
+  int tx, ty;
+};
+constexpr ShapeDesc kShapes[3] = {{32, 8}, {16, 16}, {32, 4}};
+
+// Batched mode needs one solid-class count for all members and none of the
+// per-context extras (learned start, harvest, output sweep, moving bed).
+bool ens_batchable(const ImexEnsemble* ens) {
+  const int ns = ens->members[0]->ns;
+  for (const ImexCtx* c : ens->members)
+    if (c->ns != ns || c->nw.warm || c->nw.harvest || c->post_on || c->P.topo_change_flag)
+      return false;
+  return true;
+}
+
+// Member table and tile table for tile shape `si`.
+int ens_build_tables(ImexEnsemble* ens, int si) {
+  const int n = (int)ens->members.size();
+  const int tx = kShapes[si].tx, ty = kShapes[si].ty;
+  std::vector<MemberDev> hM(n);
+  std::vector<uint32_t> tm;
+  long long tile0 = 0;
+  for (int m = 0; m < n; ++m) {
+    ImexCtx* c = ens->members[m];
+    MemberDev& d = hM[m];
+    d.P = c->P;
+    d.q = c->q;
+    d.X = c->X;
+    d.mask = c->mask;
+    d.cellinfo = c->cellinfo;
+    d.release = c->release;
+    d.Bx = c->Bx; d.By = c->By; d.Bxx = c->Bxx; d.Bxy = c->Bxy; d.Byy = c->Byy;
+    d.gc = c->gc; d.dgc = c->dgc; d.gcsx = c->gcsx; d.gcsy = c->gcsy;
+    d.ring = c->ring;
+    d.erodible = c->erodible; d.deposit = c->deposit; d.erosion = c->erosion; d.Bcent = c->Bcent;
+    d.clk = c->clk;
+    d.W = c->nw;
+    d.exchange = erosion_active(c) ? 1 : 0;
+    d.tiles_x = (c->P.nx + tx - 1) / tx;
+    const long long tiles = (long long)d.tiles_x * ((c->P.ny + ty - 1) / ty);
+    d.tile0 = tile0;
+    tm.insert(tm.end(), (size_t)tiles, (uint32_t)m);
+    tile0 += tiles;
+  }
+  if (tile0 > (long long)UINT32_MAX) return ens_fail(ens, IMEX_EUNSUPPORTED, "too many tiles");
+  if (!ens->dM) CKE(cudaMalloc((void**)&ens->dM, sizeof(MemberDev) * n));
+  if (!ens->list_off) CKE(cudaMalloc((void**)&ens->list_off, sizeof(unsigned long long) * (n + 1)));
+  if (!ens->n_active) CKE(cudaMalloc((void**)&ens->n_active, sizeof(unsigned int)));
+  if ((size_t)tile0 > ens->tile_cap) {
+    if (ens->tile_member) cudaFree(ens->tile_member);
+    if (ens->active) cudaFree(ens->active);
+    ens->tile_member = nullptr;
+    ens->active = nullptr;
+    CKE(cudaMalloc((void**)&ens->tile_member, sizeof(uint32_t) * tile0));
+    CKE(cudaMalloc((void**)&ens->active, sizeof(uint32_t) * tile0));
+    ens->tile_cap = (size_t)tile0;
+  }
+  CKE(cudaMemcpy(ens->dM, hM.data(), sizeof(MemberDev) * n, cudaMemcpyHostToDevice));
+  CKE(cudaMemcpy(ens->tile_member, tm.data(), sizeof(uint32_t) * tile0, cudaMemcpyHostToDevice));
+  ens->n_tiles = tile0;
+  ens->batch_shape = si;
+  return IMEX_OK;
+}
+
+int sm_count(int device) {
+  int n = 148;
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device);
+  return n > 0 ? n : 148;
+}
+
+// One batched step of every member on ens->root.
+template <int NS, class TS>
+cudaError_t ens_enqueue_batch_ns(ImexEnsemble* ens) {
+  const int n = (int)ens->members.size();
+  const int sms = sm_count(ens->device);
+  const size_t smem = sizeof(FluxShared<NS, TS>);
+  static std::atomic<unsigned long long> attr{0};
+  if (attr_needed(attr)) {
+    cudaError_t e = cudaFuncSetAttribute(kb_flux<NS, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(kb_flux<NS, TS>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
+    attr_done(attr);
+  }
+  cudaStream_t st = ens->root;
+  const int mgrid = (n + 127) / 128;
+  const long long tiles = ens->n_tiles;
+  const int tx = TS::TX, ty = TS::TY;
+  const int any_exchange = [&] {
+    for (const ImexCtx* c : ens->members)
+      if (erosion_active(c)) return 1;
+    return 0;
+  }();
+  kb_step_begin<<<mgrid, 128, 0, st>>>(ens->dM, n, ens->n_active);
+  kb_mask<TS><<<(int)std::min<long long>(tiles, (long long)sms * 8), 256, 0, st>>>(
+      ens->dM, ens->tile_member, tiles, ens->active, ens->n_active);
+  kb_flux<NS, TS><<<(int)std::min<long long>(tiles, (long long)sms * flux_min_blocks<NS, TS>()),
+                    TS::THREADS, smem, st>>>(ens->dM, ens->tile_member, ens->active,
+                                             ens->n_active);
+  kb_dt_clip<<<mgrid, 128, 0, st>>>(ens->dM, n);
+  kb_stage2_first<NS><<<(int)std::min<long long>(tiles, (long long)sms * IMEX_FIRST_MINB),
+                        STAGE2_THREADS, 0, st>>>(ens->dM, ens->tile_member, ens->active,
+                                                 ens->n_active, tx, ty);
+  for (int pass = 0; pass < 3; ++pass) {
+    kb_list_offsets<<<1, 1024, 0, st>>>(ens->dM, n, pass, ens->list_off);
+    if (pass < 2)
+      kb_stage2_iter<NS><<<sms * IMEX_STAGE2_MINB, STAGE2_THREADS, 0, st>>>(ens->dM, n,
+                                                                              ens->list_off, pass + 2);
+    else
+      kb_stage2_tail<NS><<<sms * IMEX_STAGE2_MINB, STAGE2_THREADS, 0, st>>>(ens->dM, n,
+                                                                              ens->list_off);
+  }
+  kb_stage2_post<NS><<<(int)std::min<long long>(tiles, (long long)sms * 8), STAGE2_THREADS, 0,
+                       st>>>(ens->dM, ens->tile_member, ens->active, ens->n_active, tx, ty);
+  if (any_exchange)
+    kb_erosion<NS><<<(int)std::min<long long>(tiles, (long long)sms * IMEX_EROSION_MINB), 128, 0,
+                     st>>>(ens->dM, ens->tile_member, ens->active, ens->n_active, tx, ty);
+  kb_step_end<<<mgrid, 128, 0, st>>>(ens->dM, n);
+  ens->batch_launches = 13 + any_exchange;
+  return cudaGetLastError();
+}
+
+template <int NS>
+cudaError_t ens_enqueue_batch_shape(ImexEnsemble* ens, int si) {
+  switch (si) {
+    case 0: return ens_enqueue_batch_ns<NS, Shape32x8>(ens);
+    case 1: return ens_enqueue_batch_ns<NS, Shape16x16>(ens);
+    default: return ens_enqueue_batch_ns<NS, Shape32x4>(ens);
+  }
+}
+
+cudaError_t ens_enqueue_batch(ImexEnsemble* ens, int si) {
+  switch (ens->members[0]->ns) {
+    case 1: return ens_enqueue_batch_shape<1>(ens, si);
+    case 2: return ens_enqueue_batch_shape<2>(ens, si);
+    case 3: return ens_enqueue_batch_shape<3>(ens, si);
+    default: return ens_enqueue_batch_shape<4>(ens, si);
+  }
+}
+
+// Capture one batched step (tile shape si) into ens->graph.
+int ens_build_batch_graph(ImexEnsemble* ens, int si) {
+  ens_drop_graph(ens);
+  if (ens->batch_shape != si) {
+    int r = ens_build_tables(ens, si);
+    if (r) return r;
+  }
+  CKE(cudaStreamBeginCapture(ens->root, cudaStreamCaptureModeThreadLocal));
+  cudaError_t err = ens_enqueue_batch(ens, si);
+  cudaGraph_t g = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(ens->root, &g);
+  if (err != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return ens_fail(ens, IMEX_ECUDA, cudaGetErrorString(err));
+  }
+  if (e2 != cudaSuccess) return ens_fail(ens, IMEX_ECUDA, cudaGetErrorString(e2));
+  ens->graph = g;
+  CKE(cudaGraphInstantiate(&ens->exec, g, 0));
+  ens->step_launches.assign(ens->members.size(), ens->batch_launches);
+  ens->graph_shape = si;
+  return IMEX_OK;
+}
 
 void ens_drop_graph(ImexEnsemble* ens) {
   if (ens->exec) cudaGraphExecDestroy(ens->exec);
@@ -1612,6 +1796,7 @@ int ens_build_graph(ImexEnsemble* ens, int k) {
   if (e2 != cudaSuccess) return ens_fail(ens, IMEX_ECUDA, cudaGetErrorString(e2));
   ens->graph = g;
   CKE(cudaGraphInstantiate(&ens->exec, g, 0));
+  ens->graph_shape = -1;
   // the capture counted each member's kernels once; replays count them
   ens->step_launches.assign(n, 0);
   for (int m = 0; m < n; ++m) {
@@ -1683,6 +1868,11 @@ int imex_gpu_ensemble_destroy(ImexEnsemble* ens) {
   for (cudaEvent_t e : ens->join) cudaEventDestroy(e);
   if (ens->fork) cudaEventDestroy(ens->fork);
   if (ens->root) cudaStreamDestroy(ens->root);
+  if (ens->dM) cudaFree(ens->dM);
+  if (ens->tile_member) cudaFree(ens->tile_member);
+  if (ens->active) cudaFree(ens->active);
+  if (ens->n_active) cudaFree(ens->n_active);
+  if (ens->list_off) cudaFree(ens->list_off);
   for (ImexCtx* c : ens->members) imex_gpu_destroy(c);
   delete ens;
   return IMEX_OK;
@@ -1702,8 +1892,47 @@ int imex_gpu_ensemble_advance(ImexEnsemble* ens, int n_steps, int* first_bad_mem
   for (ImexCtx* c : ens->members) CKE(cudaStreamSynchronize(c->stream));
   const int nmem = (int)ens->members.size();
   int done = 0;
+  if (ens_batchable(ens)) {
+    // batched mode; tuning: one real step per candidate tile shape
+    constexpr int n_shapes = (int)(sizeof(kShapes) / sizeof(kShapes[0]));
+    while (ens->shape < 0 && done < n_steps) {
+      const int si = (int)ens->tried_shape.size();
+      if (si >= n_shapes) {
+        size_t best = 0;
+        for (size_t i = 1; i < ens->tried_shape_ms.size(); ++i)
+          if (ens->tried_shape_ms[i] < ens->tried_shape_ms[best]) best = i;
+        ens->shape = ens->tried_shape[best];
+        break;
+      }
+      int r = ens_build_batch_graph(ens, si);
+      if (r) return r;
+      float ms = 0.0f;
+      r = ens_replay(ens, &ms);
+      if (r) return r;
+      ens->tried_shape.push_back(si);
+      ens->tried_shape_ms.push_back(ms);
+      ++done;
+    }
+    if (done < n_steps && ens->shape < 0) {
+      // fewer steps than shapes: keep the best so far
+      size_t best = 0;
+      for (size_t i = 1; i < ens->tried_shape_ms.size(); ++i)
+        if (ens->tried_shape_ms[i] < ens->tried_shape_ms[best]) best = i;
+      ens->shape = ens->tried_shape[best];
+    }
+    if (done < n_steps) {
+      if (!ens->exec || ens->batch_shape != ens->shape || ens->graph_shape != ens->shape) {
+        int r = ens_build_batch_graph(ens, ens->shape);
+        if (r) return r;
+      }
+      for (; done < n_steps; ++done) {
+        int r = ens_replay(ens, nullptr);
+        if (r) return r;
+      }
+    }
+  }
   // tuning: one real step per candidate stream count
-  while (ens->k_streams == 0 && done < n_steps) {
+  while (!ens_batchable(ens) && ens->k_streams == 0 && done < n_steps) {
     int k = ens->tried_k.empty() ? 1 : ens->tried_k.back() * 2;
     if (k > std::min(nmem, ENS_MAX_STREAMS)) {
       size_t best = 0;
@@ -1722,7 +1951,8 @@ int imex_gpu_ensemble_advance(ImexEnsemble* ens, int n_steps, int* first_bad_mem
     ++done;
   }
   if (done < n_steps) {
-    if (!ens->exec || ens->tried_k.empty() || ens->tried_k.back() != ens->k_streams) {
+    if (!ens->exec || ens->graph_shape >= 0 || ens->tried_k.empty() ||
+        ens->tried_k.back() != ens->k_streams) {
       int r = ens_build_graph(ens, ens->k_streams);
       if (r) return r;
       ens->tried_k.push_back(ens->k_streams);
@@ -1759,6 +1989,21 @@ int imex_gpu_ensemble_tuning(ImexEnsemble* ens, int* k_streams, int* n_tried, in
       if (tried_ms) tried_ms[n] = ens->tried_ms[i];
     }
     ++n;
+  }
+  if (n_tried) *n_tried = n;
+  return IMEX_OK;
+}
+
+int imex_gpu_ensemble_tile_shape(ImexEnsemble* ens, int* tx, int* ty, int* n_tried,
+                                 int* tried_tx, int* tried_ty, float* tried_ms, int cap) {
+  if (!ens) return IMEX_EINVAL;
+  if (tx) *tx = ens->shape >= 0 ? kShapes[ens->shape].tx : 0;
+  if (ty) *ty = ens->shape >= 0 ? kShapes[ens->shape].ty : 0;
+  const int n = (int)ens->tried_shape.size();
+  for (int i = 0; i < n && i < cap; ++i) {
+    if (tried_tx) tried_tx[i] = kShapes[ens->tried_shape[i]].tx;
+    if (tried_ty) tried_ty[i] = kShapes[ens->tried_shape[i]].ty;
+    if (tried_ms) tried_ms[i] = ens->tried_shape_ms[i];
   }
   if (n_tried) *n_tried = n;
   return IMEX_OK;

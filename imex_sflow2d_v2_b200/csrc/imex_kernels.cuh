@@ -1407,37 +1407,23 @@ __device__ __forceinline__ int newton_plain(const DevParams& P, const NewtonWork
   return it > NEWTON_MAX_IT ? NEWTON_MAX_IT : it;
 }
 
-// k_stage2_first: 80 registers (6 blocks of 128 per SM) measured faster
-// than 64 with its larger spill set.
-#ifndef IMEX_FIRST_MINB
-#define IMEX_FIRST_MINB 6
-#endif
+// Stage 2 up to Newton iteration 1 for one lane's cell (plane index c; the
+// lane takes part in the warp's list appends whether or not it has a cell).
 template <int NS>
-__global__ void __launch_bounds__(STAGE2_THREADS, IMEX_FIRST_MINB)
-    k_stage2_first(const __grid_constant__ DevParams Pp, const double* __restrict__ q,
-                   const double* __restrict__ X, const uint8_t* __restrict__ mask,
-                   const double* __restrict__ Bx, const double* __restrict__ By,
-                   const double* __restrict__ Bxx, const double* __restrict__ Bxy,
-                   const double* __restrict__ Byy, const double* __restrict__ gc, NewtonWork W,
-                   DevClock* clk) {
-  const DevParams& P = Pp;
+__device__ __forceinline__ void stage2_first_lane(
+    const DevParams& P, const double* __restrict__ q, const double* __restrict__ X,
+    const uint8_t* __restrict__ mask, const double* __restrict__ Bx,
+    const double* __restrict__ By, const double* __restrict__ Bxx,
+    const double* __restrict__ Bxy, const double* __restrict__ Byy,
+    const double* __restrict__ gc, NewtonWork W, DevClock* clk, double dt, bool valid,
+    size_t c, unsigned long long& cells, unsigned long long& it_sum,
+    unsigned long long& maxit) {
   constexpr int NV = 4 + NS, NP = 6 + NS;
-  const int nx = P.nx;
-  const long long ncell = (long long)nx * P.ny;
   const size_t N = (size_t)P.plane;
-  const double dt = clk->dt;
-  unsigned long long cells = 0, it_sum = 0, maxit = 0;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < ncell;
-       base += stride) {
-    const long long g = base + (threadIdx.x & 31);
-    size_t c = 0;
-    bool go_on = false, warm_cell = false;
-    int fin = 0;
-    float fw[WARM_IN];
-    if (g < ncell) {
-      const int j = (int)(g % nx), k = (int)(g / nx);
-      c = (size_t)k * P.pitch + j;
+  bool go_on = false, warm_cell = false;
+  int fin = 0;
+  float fw[WARM_IN];
+  if (valid) {
       if (mask[c]) {
         double q0[NV], qfv[NV], Xc[NV];
 #pragma unroll
@@ -1528,41 +1514,68 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_FIRST_MINB)
         }
       }
     }
-    newton_finish_stats(clk, fin, it_sum, maxit);
-    list_append(go_on, (uint32_t)c, W.list[0], &clk->nw_count[0]);
-    if (W.warm) {
-      const unsigned int slot = list_append(warm_cell, (uint32_t)c, W.wlist, &clk->nw_count[3]);
-      if (warm_cell) {
+  newton_finish_stats(clk, fin, it_sum, maxit);
+  list_append(go_on, (uint32_t)c, W.list[0], &clk->nw_count[0]);
+  if (W.warm) {
+    const unsigned int slot = list_append(warm_cell, (uint32_t)c, W.wlist, &clk->nw_count[3]);
+    if (warm_cell) {
 #pragma unroll
-        for (int i = 0; i < WARM_IN; ++i) W.feat[(size_t)slot * WARM_IN + i] = fw[i];
-      }
+      for (int i = 0; i < WARM_IN; ++i) W.feat[(size_t)slot * WARM_IN + i] = fw[i];
     }
+  }
+}
+
+// k_stage2_first: 80 registers (6 blocks of 128 per SM) measured faster
+// than 64 with its larger spill set.
+#ifndef IMEX_FIRST_MINB
+#define IMEX_FIRST_MINB 6
+#endif
+template <int NS>
+__global__ void __launch_bounds__(STAGE2_THREADS, IMEX_FIRST_MINB)
+    k_stage2_first(const __grid_constant__ DevParams Pp, const double* __restrict__ q,
+                   const double* __restrict__ X, const uint8_t* __restrict__ mask,
+                   const double* __restrict__ Bx, const double* __restrict__ By,
+                   const double* __restrict__ Bxx, const double* __restrict__ Bxy,
+                   const double* __restrict__ Byy, const double* __restrict__ gc, NewtonWork W,
+                   DevClock* clk) {
+  const DevParams& P = Pp;
+  const int nx = P.nx;
+  const long long ncell = (long long)nx * P.ny;
+  const double dt = clk->dt;
+  unsigned long long cells = 0, it_sum = 0, maxit = 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < ncell;
+       base += stride) {
+    const long long g = base + (threadIdx.x & 31);
+    const bool valid = g < ncell;
+    const size_t c = valid ? (size_t)(g / nx) * P.pitch + (size_t)(g % nx) : 0;
+    stage2_first_lane<NS>(P, q, X, mask, Bx, By, Bxx, Bxy, Byy, gc, W, clk, dt, valid, c, cells,
+                          it_sum, maxit);
   }
   newton_flush_stats(clk, cells, it_sum, 0, maxit);
 }
 
-// One Newton iteration (nl_iter = 2 or 3) for the cells of list `in`.
+// One Newton iteration (nl_iter = 2 or 3) for entry e of list nl_iter-2
+// (valid: e is inside the list); the lane takes part in the warp's list
+// appends whether or not it has a cell.
 template <int NS>
-__global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
-    k_stage2_iter(const __grid_constant__ DevParams Pp, const double* __restrict__ q,
-                  const double* __restrict__ Bx, const double* __restrict__ By, NewtonWork W,
-                  DevClock* clk, int nl_iter) {
-  const DevParams& P = Pp;
+__device__ __forceinline__ void stage2_iter_lane(const DevParams& P, const double* __restrict__ q,
+                                                 const double* __restrict__ Bx,
+                                                 const double* __restrict__ By, NewtonWork W,
+                                                 DevClock* clk, double dt, int nl_iter,
+                                                 bool valid, long long e,
+                                                 unsigned long long& it_sum,
+                                                 unsigned long long& maxit,
+                                                 unsigned long long& trials) {
   constexpr int NV = 4 + NS;
   const size_t N = (size_t)P.plane;
-  const double dt = clk->dt;
   const uint32_t* in = W.list[nl_iter - 2];
   uint32_t* out = W.list[nl_iter - 1];
-  const long long n = (long long)clk->nw_count[nl_iter - 2];
-  unsigned long long it_sum = 0, maxit = 0, trials = 0;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n;
-       base += stride) {
-    const long long e = base + (threadIdx.x & 31);
+  {
     uint32_t c = 0;
     bool go_on = false, fb = false;
     int fin = 0;
-    if (e < n) {
+    if (valid) {
       c = in[e];
       double q0[NV], Rj[NV], qj_org[NV], qj_rel[NV], rt[NV], qj[NV], scal_f;
 #pragma unroll
@@ -1607,29 +1620,42 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
     list_append(go_on, c, out, &clk->nw_count[nl_iter - 1]);
     if (W.warm) list_append(fb, c, W.flist, &clk->nw_fb);
   }
-  newton_flush_stats(clk, 0, it_sum, trials, maxit);
 }
 
-// Iterations 4..100 for the cells of list 2.
 template <int NS>
 __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
-    k_stage2_tail(const __grid_constant__ DevParams Pp, const double* __restrict__ q,
+    k_stage2_iter(const __grid_constant__ DevParams Pp, const double* __restrict__ q,
                   const double* __restrict__ Bx, const double* __restrict__ By, NewtonWork W,
-                  DevClock* clk) {
+                  DevClock* clk, int nl_iter) {
   const DevParams& P = Pp;
-  constexpr int NV = 4 + NS;
-  const size_t N = (size_t)P.plane;
   const double dt = clk->dt;
-  const long long n = (long long)clk->nw_count[2];
+  const long long n = (long long)clk->nw_count[nl_iter - 2];
   unsigned long long it_sum = 0, maxit = 0, trials = 0;
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n;
        base += stride) {
     const long long e = base + (threadIdx.x & 31);
+    stage2_iter_lane<NS>(P, q, Bx, By, W, clk, dt, nl_iter, e < n, e, it_sum, maxit, trials);
+  }
+  newton_flush_stats(clk, 0, it_sum, trials, maxit);
+}
+
+// Iterations 4..100 for entry e of list 2.
+template <int NS>
+__device__ __forceinline__ void stage2_tail_lane(const DevParams& P, const double* __restrict__ q,
+                                                 const double* __restrict__ Bx,
+                                                 const double* __restrict__ By, NewtonWork W,
+                                                 DevClock* clk, double dt, bool valid,
+                                                 long long e, unsigned long long& it_sum,
+                                                 unsigned long long& maxit,
+                                                 unsigned long long& trials) {
+  constexpr int NV = 4 + NS;
+  const size_t N = (size_t)P.plane;
+  {
     int fin = 0;
     bool fb = false;
     uint32_t c = 0;
-    if (e < n) {
+    if (valid) {
       c = W.list[2][e];
       double q0[NV], Rj[NV], qj_org[NV], qj_rel[NV], rt[NV], qj[NV], scal_f;
 #pragma unroll
@@ -1666,6 +1692,23 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
     }
     newton_finish_stats(clk, fin, it_sum, maxit);
     if (W.warm) list_append(fb, c, W.flist, &clk->nw_fb);
+  }
+}
+
+template <int NS>
+__global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
+    k_stage2_tail(const __grid_constant__ DevParams Pp, const double* __restrict__ q,
+                  const double* __restrict__ Bx, const double* __restrict__ By, NewtonWork W,
+                  DevClock* clk) {
+  const DevParams& P = Pp;
+  const double dt = clk->dt;
+  const long long n = (long long)clk->nw_count[2];
+  unsigned long long it_sum = 0, maxit = 0, trials = 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n;
+       base += stride) {
+    const long long e = base + (threadIdx.x & 31);
+    stage2_tail_lane<NS>(P, q, Bx, By, W, clk, dt, e < n, e, it_sum, maxit, trials);
   }
   newton_flush_stats(clk, 0, it_sum, trials, maxit);
 }
@@ -1866,20 +1909,14 @@ __global__ void __launch_bounds__(128)
 // Sign guard after Newton (src/solver_2d.f90:1238-1255) and assemble_sol
 // (src/solver_2d.f90:1339-1626).
 template <int NS>
-__global__ void __launch_bounds__(STAGE2_THREADS)
-    k_stage2_post(const __grid_constant__ DevParams Pp, double* __restrict__ q,
-                  const uint8_t* __restrict__ mask, const uint8_t* __restrict__ cellinfo,
-                  NewtonWork W, DevClock* clk) {
-  const DevParams& P = Pp;
+__device__ __forceinline__ void stage2_post_cell(const DevParams& P, double* __restrict__ q,
+                                                 const uint8_t* __restrict__ cellinfo,
+                                                 NewtonWork W, DevClock* clk, int j, int k) {
   constexpr int NV = 4 + NS, NP = 6 + NS;
   const int nx = P.nx, ny = P.ny;
-  const long long ncell = (long long)nx * ny;
   const size_t N = (size_t)P.plane;
-  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < ncell;
-       g += (long long)gridDim.x * blockDim.x) {
-    const int j = (int)(g % nx), k = (int)(g / nx);
-    const size_t c = (size_t)k * P.pitch + j;
-    if (!mask[c]) continue;
+  const size_t c = (size_t)k * P.pitch + j;
+  {
     double qc[NV];
 #pragma unroll
     for (int i = 0; i < NV; ++i) qc[i] = W.x[c + i * N];
@@ -1953,23 +1990,36 @@ __global__ void __launch_bounds__(STAGE2_THREADS)
   }
 }
 
-// Stand-alone erosion/deposition pass (imex_gpu_erosion_deposition).
 template <int NS>
-__global__ void __launch_bounds__(128, IMEX_EROSION_MINB)
-    k_erosion(const __grid_constant__ DevParams Pp, double* __restrict__ q, const uint8_t* __restrict__ mask,
-              const double* __restrict__ Bx, const double* __restrict__ By,
-              double* __restrict__ erodible, double* __restrict__ deposit,
-              double* __restrict__ erosion, double* __restrict__ Bcent, DevClock* clk) {
+__global__ void __launch_bounds__(STAGE2_THREADS)
+    k_stage2_post(const __grid_constant__ DevParams Pp, double* __restrict__ q,
+                  const uint8_t* __restrict__ mask, const uint8_t* __restrict__ cellinfo,
+                  NewtonWork W, DevClock* clk) {
   const DevParams& P = Pp;
-  constexpr int NV = 4 + NS;
   const int nx = P.nx;
   const long long ncell = (long long)nx * P.ny;
-  const double dt = clk->dt;
   for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < ncell;
        g += (long long)gridDim.x * blockDim.x) {
-    int j = (int)(g % nx), k = (int)(g / nx);
-    size_t c = (size_t)k * P.pitch + j;
-    if (!mask[c]) continue;
+    const int j = (int)(g % nx), k = (int)(g / nx);
+    if (!mask[(size_t)k * P.pitch + j]) continue;
+    stage2_post_cell<NS>(P, q, cellinfo, W, clk, j, k);
+  }
+}
+
+// Stand-alone erosion/deposition pass (imex_gpu_erosion_deposition).
+template <int NS>
+__device__ __forceinline__ void erosion_update_cell(const DevParams& P, double* __restrict__ q,
+                                                    const double* __restrict__ Bx,
+                                                    const double* __restrict__ By,
+                                                    double* __restrict__ erodible,
+                                                    double* __restrict__ deposit,
+                                                    double* __restrict__ erosion,
+                                                    double* __restrict__ Bcent, DevClock* clk,
+                                                    double dt, int j, int k) {
+  constexpr int NV = 4 + NS;
+  const int nx = P.nx;
+  const size_t c = (size_t)k * P.pitch + j;
+  {
     double qc[NV];
 #pragma unroll
     for (int i = 0; i < NV; ++i) qc[i] = q[c + (size_t)i * P.plane];
@@ -1996,6 +2046,24 @@ __global__ void __launch_bounds__(128, IMEX_EROSION_MINB)
   }
 }
 
+template <int NS>
+__global__ void __launch_bounds__(128, IMEX_EROSION_MINB)
+    k_erosion(const __grid_constant__ DevParams Pp, double* __restrict__ q, const uint8_t* __restrict__ mask,
+              const double* __restrict__ Bx, const double* __restrict__ By,
+              double* __restrict__ erodible, double* __restrict__ deposit,
+              double* __restrict__ erosion, double* __restrict__ Bcent, DevClock* clk) {
+  const DevParams& P = Pp;
+  const int nx = P.nx;
+  const long long ncell = (long long)nx * P.ny;
+  const double dt = clk->dt;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < ncell;
+       g += (long long)gridDim.x * blockDim.x) {
+    int j = (int)(g % nx), k = (int)(g / nx);
+    if (!mask[(size_t)k * P.pitch + j]) continue;
+    erosion_update_cell<NS>(P, q, Bx, By, erodible, deposit, erosion, Bcent, clk, dt, j, k);
+  }
+}
+
 // ============================================================ small kernels
 // FMA-chain throughput probe: each thread runs 8 independent chains of
 // `iters` dependent fused multiply-adds (the measured FP64 peak).
@@ -2011,7 +2079,7 @@ __global__ void k_fp64_probe(double* out, int iters, double a, double b) {
 }
 
 // Resets the per-step accumulators of the clock.
-__global__ void k_step_begin(DevClock* clk, double max_dt, int reset_cells) {
+__device__ __forceinline__ void step_begin(DevClock* clk, double max_dt, int reset_cells) {
   clk->dtmin_bits = (unsigned long long)__double_as_longlong(max_dt);
   if (reset_cells) clk->solve_cells = 0;
   clk->newton_cells = 0;
@@ -2022,14 +2090,19 @@ __global__ void k_step_begin(DevClock* clk, double max_dt, int reset_cells) {
   for (int b = 0; b < 16; ++b) clk->hist[b] = 0;
 }
 
+__global__ void k_step_begin(DevClock* clk, double max_dt, int reset_cells) {
+  step_begin(clk, max_dt, reset_cells);
+}
+
 // Empties the stage-2 Newton lists (before each stage 2).
-__global__ void k_nw_reset(DevClock* clk) {
+__device__ __forceinline__ void nw_reset(DevClock* clk) {
   for (int i = 0; i < 4; ++i) clk->nw_count[i] = 0;
   clk->nw_fb = 0;
 }
+__global__ void k_nw_reset(DevClock* clk) { nw_reset(clk); }
 
 // dt from the CFL minimum with the driver's clipping (src/IMEX_SfloW2D.f90:359-381).
-__global__ void k_dt_clip(DevClock* clk, int clip) {
+__device__ __forceinline__ void dt_clip(DevClock* clk, int clip) {
   double dt = __longlong_as_double((long long)clk->dtmin_bits);
   if (clip) {
     double t = clk->t;
@@ -2041,11 +2114,13 @@ __global__ void k_dt_clip(DevClock* clk, int clip) {
   }
   clk->dt = dt;
 }
+__global__ void k_dt_clip(DevClock* clk, int clip) { dt_clip(clk, clip); }
 
-__global__ void k_step_end(DevClock* clk) {
+__device__ __forceinline__ void step_end(DevClock* clk) {
   clk->t = clk->t + clk->dt;
   clk->steps += 1;
 }
+__global__ void k_step_end(DevClock* clk) { step_end(clk); }
 
 // Fortran AoS q(n_vars,nx,ny) <-> SoA planes.
 __global__ void k_aos_to_soa(const double* __restrict__ aos, double* __restrict__ soa, int nv,

@@ -112,6 +112,10 @@ def load_library(path=None, fast=False):
         "imex_gpu_ensemble_tuning": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int],
                                      C.c_int),
+        "imex_gpu_ensemble_tile_shape": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                          C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                          C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int],
+                                         C.c_int),
         "imex_gpu_ensemble_last_error": ([vp], C.c_char_p),
     }
     for name, (args, res) in sig.items():
@@ -371,8 +375,10 @@ class ImexSolver:
 
 
 class ImexEnsemble:
-    """Independent runs (members) advanced together on one GPU from one CUDA
-    graph per step (the reference runs one process per member,
+    """Independent runs (members) advanced together on one GPU: batched (every
+    phase one persistent kernel for all members, the step one CUDA graph),
+    or through per-member graphs forked over streams when the members cannot
+    share the batched kernels (the reference runs one process per member,
     EXAMPLES/EXAMPLE_ENSEMBLE_ETNA/launch_jobs.py).  `members` is a list of
     (params, static_arrays); member m's context is ``self.member(m)`` (an
     ImexSolver view for set_state, set_clock, get_state, stats ...)."""
@@ -423,6 +429,18 @@ class ImexEnsemble:
         tm = (C.c_float * 16)()
         self.lib.imex_gpu_ensemble_tuning(self._h, C.byref(k), C.byref(n), tk, tm, 16)
         return k.value, [(tk[i], tm[i]) for i in range(min(n.value, 16))]
+
+    def tile_shape(self):
+        """Batched mode: ((tx, ty) chosen, [((tx, ty), ms of its timed step),
+        ...]); ((0, 0), []) when the members advance through per-member
+        graphs."""
+        tx, ty, n = C.c_int(0), C.c_int(0), C.c_int(0)
+        ax = (C.c_int * 8)()
+        ay = (C.c_int * 8)()
+        ms = (C.c_float * 8)()
+        self.lib.imex_gpu_ensemble_tile_shape(self._h, C.byref(tx), C.byref(ty), C.byref(n), ax,
+                                              ay, ms, 8)
+        return (tx.value, ty.value), [((ax[i], ay[i]), ms[i]) for i in range(min(n.value, 8))]
 
     def close(self):
         if getattr(self, "_h", None):

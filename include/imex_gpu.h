@@ -344,6 +344,19 @@ int imex_gpu_harvest_data(ImexCtx* ctx, const float** x_dev, const float** y_dev
  * (results do not depend on K).  It returns the first status code found
  * (member order) and, in *first_bad_member, that member (-1: none).
  * imex_gpu_ensemble_tuning reports the chosen K and the timed candidates.
+ *
+ * When all members share one solid-class count and none uses the learned
+ * start, the harvest, the output sweep or a moving bed, the ensemble runs
+ * batched instead: every phase of the step is one persistent kernel for all
+ * members (a fixed grid walking device-built work lists: all tiles for the
+ * mask, the tiles holding a solve cell for the fluxes, stage 2 and erosion,
+ * the members' Newton lists laid end to end for the iteration passes), 13
+ * or 14 launches per step for the whole ensemble, captured once in a CUDA
+ * graph and replayed.  Its first calls time one real step with each tile
+ * shape of the mask and flux passes (32x8, 16x16, 32x4 cells) and keep the
+ * fastest; imex_gpu_ensemble_tile_shape reports the chosen shape (0x0: not
+ * batched) and the timed candidates.  Results equal each member's single
+ * run bit for bit in both modes.
  */
 typedef struct ImexEnsemble ImexEnsemble;
 int imex_gpu_ensemble_create(int n_members, const ImexParams* const* params,
@@ -353,6 +366,8 @@ int imex_gpu_ensemble_member(ImexEnsemble* ens, int m, ImexCtx** ctx);
 int imex_gpu_ensemble_advance(ImexEnsemble* ens, int n_steps, int* first_bad_member);
 int imex_gpu_ensemble_tuning(ImexEnsemble* ens, int* k_streams, int* n_tried, int* tried_k,
                              float* tried_ms, int cap);
+int imex_gpu_ensemble_tile_shape(ImexEnsemble* ens, int* tx, int* ty, int* n_tried,
+                                 int* tried_tx, int* tried_ty, float* tried_ms, int cap);
 const char* imex_gpu_ensemble_last_error(ImexEnsemble* ens);
 
 /*
