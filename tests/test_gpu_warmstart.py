@@ -67,3 +67,59 @@ def test_bad_network_costs_iterations_not_accuracy():
     assert np.isfinite(q_warm).all()
     assert rel_l1(q_plain, q_warm) <= 1e-8
     assert it_warm >= it_plain
+
+
+def test_learned_start_gain_on_radial_current():
+    """What the trained network gains on the learned-start workload's setup
+    (radial current, two solid classes, Voellmy; 256^2 here): the network is
+    trained on pairs harvested from the same run, then 10 steps are taken
+    from one state with the plain start and with the learned one.
+
+    Expected: no gain.  The solve scales its unknowns by the start
+    (q_rel = q / max(|q_start|, 1e-3), src/solver_2d.f90:1786-1798) and
+    exits on an absolute residual of 1e-10 or a relative step below machine
+    epsilon (:1964-1988), so only a start accurate to round-off saves an
+    iteration; the plain start's first full Newton step already lands
+    there.  The learned start must not cost accuracy either: no fallbacks,
+    states equal to relative L1 1e-10."""
+    from imex_sflow2d_v2_b200 import configs
+    p, st, q = configs.radial_current(nx=256, ny=256)
+    g = _developed(p, st, q, 150)
+    g.harvest_start(capacity=1 << 18, stride=1)
+    g.advance(5)
+    g.harvest_stop()
+    net = ImexMLP(seed=5)
+    n_pairs, losses = warmstart.train(net, g, epochs=6, batch=2048)
+    assert n_pairs > 10000 and losses[-1] < losses[0]
+    qs, t = g.get_state(), g.stats().t
+    g.close()
+    rec = {}
+    for mode in ("plain", "learned"):
+        r = ImexSolver(p, st)
+        r.set_state(qs, t)
+        r.set_clock(t, 1e-2)
+        if mode == "learned":
+            r.set_warmstart(net)
+        r.profile(True)
+        its = cells = fb = 0
+        for _ in range(10):
+            r.advance(1)
+            s = r.stats()
+            its += s.newton_iters
+            cells += s.newton_cells
+            fb += s.warm_fallback_cells
+        kt = r.kernel_times()
+        rec[mode] = {"iters_per_cell": its / max(1, cells), "fallback": fb,
+                     "stage2_ms": sum(kt[k][0] for k in ("stage2_first", "stage2_iter",
+                                                         "stage2_post")),
+                     "q": r.get_state(), "mask": r.get_masks()[0]}
+        r.close()
+    net.close()
+    gain = rec["plain"]["iters_per_cell"] - rec["learned"]["iters_per_cell"]
+    summary = {m: {k: v for k, v in rec[m].items() if k not in ("q", "mask")} for m in rec}
+    summary["gain_iters_per_cell"] = gain
+    print("learned vs plain:", summary)
+    assert rec["learned"]["fallback"] == 0, summary
+    assert rel_l1(rec["plain"]["q"], rec["learned"]["q"]) <= 1e-10, summary
+    assert np.array_equal(rec["plain"]["mask"], rec["learned"]["mask"]), summary
+    assert gain < 0.05, summary       # the expected sign: no gain
