@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--ens-members", type=int, default=256)
     ap.add_argument("--ens-steps", type=int, default=1000)
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--ens-compare", action="store_true",
+                    help="also time the ensemble through per-member graphs over streams")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-setup", action="store_true")
     ap.add_argument("--output-n", type=int, default=1024,
@@ -297,11 +299,34 @@ def config_rates(args, device):
     return out
 
 
+def run_ensemble_streams(args):
+    """The ensemble workload through per-member graphs over streams (the
+    mode the batched one replaces), for comparison; same timing rule."""
+    from imex_sflow2d_v2_b200 import configs
+    from imex_sflow2d_v2_b200.solver import ImexEnsemble
+    mem = configs.ensemble_members(n_members=args.ens_members)
+    ens = ImexEnsemble([(p, st) for p, st, q, s in mem])
+    ens.set_mode(per_member_graphs=True)
+    for m, (p, st, q, s) in enumerate(mem):
+        ens.member(m).set_state(q, 0.0)
+        ens.member(m).set_clock(0.0, 1e-2)
+    n_tune = 6      # stream counts 1, 2, 4, 8, 16, 32
+    ens.advance(n_tune)
+    t0 = time.perf_counter()
+    ens.advance(args.ens_steps - n_tune)
+    el = time.perf_counter() - t0
+    per_run = el * args.ens_steps / (args.ens_steps - n_tune)
+    k, tried = ens.tuning()
+    ens.close()
+    return {"seconds": per_run, "members_per_hour": args.ens_members * 3600.0 / per_run,
+            "k_streams": k, "tuning_ms_per_step": tried}
+
+
 def run_ensemble(args):
     """Batched ensemble (fourth workload): members/hour for `ens_steps` steps
-    of every member.  The first steps (one per candidate tile shape, the
-    tuner's trials; real steps of the run) are taken before the timed
-    region; the rate is scaled to all `ens_steps` steps."""
+    of every member.  The first six steps (the tuner's trials of the tile
+    shapes; real steps of the run) are taken before the timed region; the
+    rate is scaled to all `ens_steps` steps."""
     import math
     from imex_sflow2d_v2_b200 import configs
     from imex_sflow2d_v2_b200.solver import ImexEnsemble
@@ -311,7 +336,7 @@ def run_ensemble(args):
         ens.member(m).set_state(q, 0.0)
         ens.member(m).set_clock(0.0, 1e-2)
     cells = sum(p.nx * p.ny for p, *_ in mem)
-    n_tune = 3
+    n_tune = 6
     t0 = time.perf_counter()
     ens.advance(n_tune)
     tune_s = time.perf_counter() - t0
@@ -750,6 +775,8 @@ def main():
     ensemble = None
     if rank == 0 and world == 1 and not args.no_ensemble:
         ensemble = run_ensemble(args)
+        if args.ens_compare:
+            ensemble["per_member_graphs"] = run_ensemble_streams(args)
     setup = None
     if rank == 0 and world == 1 and not args.no_setup:
         setup = run_setup(args)

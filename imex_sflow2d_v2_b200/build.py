@@ -11,7 +11,8 @@ LIB_FAST = os.path.join(_HERE, "libimexgpu_fast.so")
 
 
 def sources():
-    return [os.path.join(CSRC, f) for f in ("imex_gpu.cu", "imex_kernels.cuh", "imex_batch.cuh", "imex_mlp.cuh",
+    return [os.path.join(CSRC, f) for f in ("imex_gpu.cu", "imex_batch.cu", "imex_kernels.cuh",
+                                             "imex_batch.cuh", "imex_batch_api.h", "imex_mlp.cuh",
                                              "imex_device.cuh", "imex_setup.cuh", "imex_output.cuh",
                                              "imex_fortran_fmt.h",
                                              "ipow_tables.h")] + [
@@ -30,7 +31,7 @@ def needs_build():
 
 def build(force=False, verbose=False):
     if force or needs_build():
-        cmd = ["make", "-j2", "-C", CSRC, "NVCC=/usr/local/cuda/bin/nvcc", "all"]
+        cmd = ["make", "-j4", "-C", CSRC, "NVCC=/usr/local/cuda/bin/nvcc", "all"]
         if force:
             cmd.insert(1, "-B")
         out = subprocess.run(cmd, capture_output=not verbose, text=True)

@@ -19,6 +19,7 @@
 #include "imex_kernels.cuh"
 
 namespace imex {
+inline namespace IMEX_TU_NS {
 
 // A member as the batched kernels see it (device memory).
 struct MemberDev {
@@ -37,6 +38,21 @@ struct MemberDev {
   int exchange;       // the erosion/deposition pass runs for this member
   long long tile0;    // first global tile index of the member
 };
+
+// The per-cell passes read a member's parameters from a copy in shared
+// memory, refreshed when the block (or, in the list passes, the warp) moves
+// to another member: read straight from global memory, the parameters the
+// inner loops use add load latency and registers to every pass (measured
+// 20-30% slower per pass than the single-grid kernels, whose parameters are
+// a __grid_constant__ kernel argument).
+__device__ __forceinline__ void stage_params(DevParams& dst, const DevParams& src, int tid,
+                                             int nthreads) {
+  static_assert(sizeof(DevParams) % 8 == 0 && alignof(DevParams) >= 8, "DevParams words");
+  constexpr int W = (int)(sizeof(DevParams) / 8);
+  const unsigned long long* a = reinterpret_cast<const unsigned long long*>(&src);
+  unsigned long long* b = reinterpret_cast<unsigned long long*>(&dst);
+  for (int i = tid; i < W; i += nthreads) b[i] = a[i];
+}
 
 // Position of global tile g: its member and its first cell (j0, k0).
 struct TilePos {
@@ -92,6 +108,19 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// The flux pass stages a member's parameters in shared memory too, when the
+// copy leaves the blocks per SM unchanged (kb_flux_smem: the bytes of one
+// block).
+template <int NS, class TS>
+__host__ __device__ constexpr bool flux_stages_params() {
+  return (size_t)flux_min_blocks<NS, TS>() * (sizeof(FluxShared<NS, TS>) + sizeof(DevParams) + 1024) <=
+         (size_t)228 * 1024;
+}
+template <int NS, class TS>
+__host__ __device__ constexpr size_t kb_flux_smem() {
+  return sizeof(FluxShared<NS, TS>) + (flux_stages_params<NS, TS>() ? sizeof(DevParams) : 0);
+}
+
 // Stage 1 and the CFL minimum of the active tiles.
 template <int NS, class TS>
 __global__ void __launch_bounds__(TS::THREADS, (flux_min_blocks<NS, TS>()))
@@ -99,12 +128,25 @@ __global__ void __launch_bounds__(TS::THREADS, (flux_min_blocks<NS, TS>()))
             const uint32_t* __restrict__ active, const unsigned int* __restrict__ n_active) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   FluxShared<NS, TS>& S = *reinterpret_cast<FluxShared<NS, TS>*>(smem_raw);
+  DevParams& sP = *reinterpret_cast<DevParams*>(smem_raw + sizeof(FluxShared<NS, TS>));
   const unsigned int n = *n_active;
+  const MemberDev* cur = nullptr;
   for (unsigned int a = blockIdx.x; a < n; a += gridDim.x) {
     const TilePos t = tile_pos(M, tile_member, active[a], TS::TX, TS::TY);
     const MemberDev& D = *t.D;
-    flux_tile<NS, TS>(D.P, D.q, D.mask, D.cellinfo, D.Bx, D.By, D.Bxx, D.Bxy, D.Byy, D.gc, D.dgc,
-                      D.gcsx, D.gcsy, D.ring, D.clk, D.X, t.j0, t.k0, S);
+    if constexpr (flux_stages_params<NS, TS>()) {
+      if (t.D != cur) {
+        __syncthreads();
+        stage_params(sP, D.P, threadIdx.x, blockDim.x);
+        __syncthreads();
+        cur = t.D;
+      }
+      flux_tile<NS, TS>(sP, D.q, D.mask, D.cellinfo, D.Bx, D.By, D.Bxx, D.Bxy, D.Byy, D.gc,
+                        D.dgc, D.gcsx, D.gcsy, D.ring, D.clk, D.X, t.j0, t.k0, S);
+    } else {
+      flux_tile<NS, TS>(D.P, D.q, D.mask, D.cellinfo, D.Bx, D.By, D.Bxx, D.Bxy, D.Byy, D.gc,
+                        D.dgc, D.gcsx, D.gcsy, D.ring, D.clk, D.X, t.j0, t.k0, S);
+    }
   }
 }
 
@@ -115,18 +157,26 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_FIRST_MINB)
     kb_stage2_first(const MemberDev* __restrict__ M, const uint32_t* __restrict__ tile_member,
                     const uint32_t* __restrict__ active, const unsigned int* __restrict__ n_active,
                     int tx, int ty) {
+  __shared__ DevParams sP;
   const unsigned int n = *n_active;
+  const MemberDev* cur = nullptr;
   for (unsigned int a = blockIdx.x; a < n; a += gridDim.x) {
     const TilePos t = tile_pos(M, tile_member, active[a], tx, ty);
     const MemberDev& D = *t.D;
+    if (t.D != cur) {
+      __syncthreads();
+      stage_params(sP, D.P, threadIdx.x, blockDim.x);
+      __syncthreads();
+      cur = t.D;
+    }
     const double dt = D.clk->dt;
     unsigned long long cells = 0, it_sum = 0, maxit = 0;
     for (int base = 0; base < tx * ty; base += blockDim.x) {
       const int e = base + threadIdx.x;
       const int j = t.j0 + e % tx, k = t.k0 + e / tx;
-      const bool valid = e < tx * ty && j < D.P.nx && k < D.P.ny;
-      const size_t c = valid ? (size_t)k * D.P.pitch + j : 0;
-      stage2_first_lane<NS>(D.P, D.q, D.X, D.mask, D.Bx, D.By, D.Bxx, D.Bxy, D.Byy, D.gc, D.W,
+      const bool valid = e < tx * ty && j < sP.nx && k < sP.ny;
+      const size_t c = valid ? (size_t)k * sP.pitch + j : 0;
+      stage2_first_lane<NS>(sP, D.q, D.X, D.mask, D.Bx, D.By, D.Bxx, D.Bxy, D.Byy, D.gc, D.W,
                             D.clk, dt, valid, c, cells, it_sum, maxit);
     }
     newton_flush_stats(D.clk, cells, it_sum, 0, maxit);
@@ -187,16 +237,25 @@ template <int NS>
 __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
     kb_stage2_iter(const MemberDev* __restrict__ M, int n, const unsigned long long* __restrict__ off,
                    int nl_iter) {
+  __shared__ DevParams sP[STAGE2_THREADS / 32];
+  DevParams& wP = sP[threadIdx.x >> 5];
+  int cur = -1;
   const unsigned long long total = off[n];
   const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
   for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31);
        base < total; base += stride) {
     const int m = list_member(off, n, base);
     const MemberDev& D = M[m];
+    if (m != cur) {
+      __syncwarp();
+      stage_params(wP, D.P, threadIdx.x & 31, 32);
+      __syncwarp();
+      cur = m;
+    }
     const long long e = (long long)(base - off[m]) + (threadIdx.x & 31);
     const bool valid = e < (long long)D.clk->nw_count[nl_iter - 2];
     unsigned long long it_sum = 0, maxit = 0, trials = 0;
-    stage2_iter_lane<NS>(D.P, D.q, D.Bx, D.By, D.W, D.clk, D.clk->dt, nl_iter, valid, e, it_sum,
+    stage2_iter_lane<NS>(wP, D.q, D.Bx, D.By, D.W, D.clk, D.clk->dt, nl_iter, valid, e, it_sum,
                          maxit, trials);
     newton_flush_stats(D.clk, 0, it_sum, trials, maxit);
   }
@@ -206,16 +265,25 @@ __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
 template <int NS>
 __global__ void __launch_bounds__(STAGE2_THREADS, IMEX_STAGE2_MINB)
     kb_stage2_tail(const MemberDev* __restrict__ M, int n, const unsigned long long* __restrict__ off) {
+  __shared__ DevParams sP[STAGE2_THREADS / 32];
+  DevParams& wP = sP[threadIdx.x >> 5];
+  int cur = -1;
   const unsigned long long total = off[n];
   const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
   for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31);
        base < total; base += stride) {
     const int m = list_member(off, n, base);
     const MemberDev& D = M[m];
+    if (m != cur) {
+      __syncwarp();
+      stage_params(wP, D.P, threadIdx.x & 31, 32);
+      __syncwarp();
+      cur = m;
+    }
     const long long e = (long long)(base - off[m]) + (threadIdx.x & 31);
     const bool valid = e < (long long)D.clk->nw_count[2];
     unsigned long long it_sum = 0, maxit = 0, trials = 0;
-    stage2_tail_lane<NS>(D.P, D.q, D.Bx, D.By, D.W, D.clk, D.clk->dt, valid, e, it_sum, maxit,
+    stage2_tail_lane<NS>(wP, D.q, D.Bx, D.By, D.W, D.clk, D.clk->dt, valid, e, it_sum, maxit,
                          trials);
     newton_flush_stats(D.clk, 0, it_sum, trials, maxit);
   }
@@ -227,14 +295,22 @@ __global__ void __launch_bounds__(STAGE2_THREADS)
     kb_stage2_post(const MemberDev* __restrict__ M, const uint32_t* __restrict__ tile_member,
                    const uint32_t* __restrict__ active, const unsigned int* __restrict__ n_active,
                    int tx, int ty) {
+  __shared__ DevParams sP;
   const unsigned int n = *n_active;
+  const MemberDev* cur = nullptr;
   for (unsigned int a = blockIdx.x; a < n; a += gridDim.x) {
     const TilePos t = tile_pos(M, tile_member, active[a], tx, ty);
     const MemberDev& D = *t.D;
+    if (t.D != cur) {
+      __syncthreads();
+      stage_params(sP, D.P, threadIdx.x, blockDim.x);
+      __syncthreads();
+      cur = t.D;
+    }
     for (int e = threadIdx.x; e < tx * ty; e += blockDim.x) {
       const int j = t.j0 + e % tx, k = t.k0 + e / tx;
-      if (j >= D.P.nx || k >= D.P.ny || !D.mask[(size_t)k * D.P.pitch + j]) continue;
-      stage2_post_cell<NS>(D.P, D.q, D.cellinfo, D.W, D.clk, j, k);
+      if (j >= sP.nx || k >= sP.ny || !D.mask[(size_t)k * sP.pitch + j]) continue;
+      stage2_post_cell<NS>(sP, D.q, D.cellinfo, D.W, D.clk, j, k);
     }
   }
 }
@@ -246,19 +322,28 @@ __global__ void __launch_bounds__(128, IMEX_EROSION_MINB)
     kb_erosion(const MemberDev* __restrict__ M, const uint32_t* __restrict__ tile_member,
                const uint32_t* __restrict__ active, const unsigned int* __restrict__ n_active,
                int tx, int ty) {
+  __shared__ DevParams sP;
   const unsigned int n = *n_active;
+  const MemberDev* cur = nullptr;
   for (unsigned int a = blockIdx.x; a < n; a += gridDim.x) {
     const TilePos t = tile_pos(M, tile_member, active[a], tx, ty);
     const MemberDev& D = *t.D;
     if (!D.exchange) continue;
+    if (t.D != cur) {
+      __syncthreads();
+      stage_params(sP, D.P, threadIdx.x, blockDim.x);
+      __syncthreads();
+      cur = t.D;
+    }
     const double dt = D.clk->dt;
     for (int e = threadIdx.x; e < tx * ty; e += blockDim.x) {
       const int j = t.j0 + e % tx, k = t.k0 + e / tx;
-      if (j >= D.P.nx || k >= D.P.ny || !D.mask[(size_t)k * D.P.pitch + j]) continue;
-      erosion_update_cell<NS>(D.P, D.q, D.Bx, D.By, D.erodible, D.deposit, D.erosion, D.Bcent,
+      if (j >= sP.nx || k >= sP.ny || !D.mask[(size_t)k * sP.pitch + j]) continue;
+      erosion_update_cell<NS>(sP, D.q, D.Bx, D.By, D.erodible, D.deposit, D.erosion, D.Bcent,
                               D.clk, dt, j, k);
     }
   }
 }
 
+}  // namespace IMEX_TU_NS
 }  // namespace imex

@@ -69,7 +69,14 @@
 #define IMEX_DIV_FN IMEX_HD
 #endif
 
+#ifndef IMEX_TU_NS
+#error "define IMEX_TU_NS (the translation unit's namespace) before including the kernels"
+#endif
 namespace imex {
+// The library is built from more than one translation unit, each with its
+// own copy of these kernels and device functions: an inline namespace named
+// per unit keeps their symbols apart.
+inline namespace IMEX_TU_NS {
 
 constexpr double EPS = 2.220446049250313e-16;  // EPSILON(1.0_wp)
 constexpr int MAXS = 4;
@@ -865,4 +872,5 @@ IMEX_SETTLE_FN double settling_velocity(const DevParams& P, double diam, double 
   return sv;
 }
 
+}  // namespace IMEX_TU_NS
 }  // namespace imex

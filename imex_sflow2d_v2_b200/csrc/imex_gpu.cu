@@ -7,6 +7,9 @@
 // body on the device and can replay it from a captured CUDA graph.
 #include <cuda_runtime.h>
 
+// namespace of this unit's copy of the kernels (imex_device.cuh)
+#define IMEX_TU_NS tu_gpu
+
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -18,7 +21,7 @@
 
 #include "../../include/imex_gpu.h"
 #include "imex_kernels.cuh"
-#include "imex_batch.cuh"
+#include "imex_batch_api.h"
 #include "imex_mlp.cuh"
 #include "imex_setup.cuh"
 #include "imex_output.cuh"
@@ -1554,7 +1557,7 @@ struct ImexEnsemble {
   int batch_shape = -1;              // shape the device tables are built for
   std::vector<int> tried_shape;
   std::vector<float> tried_shape_ms;
-  MemberDev* dM = nullptr;
+  void* dM = nullptr;                // device member table (imex_batch_api.h)
   uint32_t* tile_member = nullptr;
   uint32_t* active = nullptr;
   unsigned int* n_active = nullptr;
@@ -1563,6 +1566,7 @@ struct ImexEnsemble {
   size_t tile_cap = 0;               // capacity of tile_member / active
   int64_t batch_launches = 0;        // kernels in one batched step
   int graph_shape = -1;              // tile shape of the captured graph (-1: per-member graph)
+  int mode = 0;                      // 0 batched when possible, 2 per-member graphs
 };
 
 namespace {
@@ -1602,13 +1606,17 @@ bool ens_batchable(const ImexEnsemble* ens) {
 int ens_build_tables(ImexEnsemble* ens, int si) {
   const int n = (int)ens->members.size();
   const int tx = kShapes[si].tx, ty = kShapes[si].ty;
-  std::vector<MemberDev> hM(n);
+  const size_t mb = imex_batch::member_bytes();
+  std::vector<unsigned char> hM(mb * n);
   std::vector<uint32_t> tm;
   long long tile0 = 0;
   for (int m = 0; m < n; ++m) {
     ImexCtx* c = ens->members[m];
-    MemberDev& d = hM[m];
-    d.P = c->P;
+    imex_batch::MemberSrc d{};
+    d.params = &c->P;
+    d.params_bytes = sizeof(DevParams);
+    d.newton_work = &c->nw;
+    d.newton_work_bytes = sizeof(NewtonWork);
     d.q = c->q;
     d.X = c->X;
     d.mask = c->mask;
@@ -1619,16 +1627,17 @@ int ens_build_tables(ImexEnsemble* ens, int si) {
     d.ring = c->ring;
     d.erodible = c->erodible; d.deposit = c->deposit; d.erosion = c->erosion; d.Bcent = c->Bcent;
     d.clk = c->clk;
-    d.W = c->nw;
     d.exchange = erosion_active(c) ? 1 : 0;
     d.tiles_x = (c->P.nx + tx - 1) / tx;
     const long long tiles = (long long)d.tiles_x * ((c->P.ny + ty - 1) / ty);
     d.tile0 = tile0;
+    if (!imex_batch::fill_member(hM.data() + mb * m, d))
+      return ens_fail(ens, IMEX_EINVAL, "member record layout differs between units");
     tm.insert(tm.end(), (size_t)tiles, (uint32_t)m);
     tile0 += tiles;
   }
   if (tile0 > (long long)UINT32_MAX) return ens_fail(ens, IMEX_EUNSUPPORTED, "too many tiles");
-  if (!ens->dM) CKE(cudaMalloc((void**)&ens->dM, sizeof(MemberDev) * n));
+  if (!ens->dM) CKE(cudaMalloc(&ens->dM, mb * n));
   if (!ens->list_off) CKE(cudaMalloc((void**)&ens->list_off, sizeof(unsigned long long) * (n + 1)));
   if (!ens->n_active) CKE(cudaMalloc((void**)&ens->n_active, sizeof(unsigned int)));
   if ((size_t)tile0 > ens->tile_cap) {
@@ -1640,7 +1649,7 @@ int ens_build_tables(ImexEnsemble* ens, int si) {
     CKE(cudaMalloc((void**)&ens->active, sizeof(uint32_t) * tile0));
     ens->tile_cap = (size_t)tile0;
   }
-  CKE(cudaMemcpy(ens->dM, hM.data(), sizeof(MemberDev) * n, cudaMemcpyHostToDevice));
+  CKE(cudaMemcpy(ens->dM, hM.data(), mb * n, cudaMemcpyHostToDevice));
   CKE(cudaMemcpy(ens->tile_member, tm.data(), sizeof(uint32_t) * tile0, cudaMemcpyHostToDevice));
   ens->n_tiles = tile0;
   ens->batch_shape = si;
@@ -1653,76 +1662,27 @@ int sm_count(int device) {
   return n > 0 ? n : 148;
 }
 
-// One batched step of every member on ens->root.
-template <int NS, class TS>
-cudaError_t ens_enqueue_batch_ns(ImexEnsemble* ens) {
-  const int n = (int)ens->members.size();
-  const int sms = sm_count(ens->device);
-  const size_t smem = sizeof(FluxShared<NS, TS>);
-  static std::atomic<unsigned long long> attr{0};
-  if (attr_needed(attr)) {
-    cudaError_t e = cudaFuncSetAttribute(kb_flux<NS, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(kb_flux<NS, TS>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             (int)cudaSharedmemCarveoutMaxShared);
-    if (e != cudaSuccess) return e;
-    attr_done(attr);
-  }
-  cudaStream_t st = ens->root;
-  const int mgrid = (n + 127) / 128;
-  const long long tiles = ens->n_tiles;
-  const int tx = TS::TX, ty = TS::TY;
-  const int any_exchange = [&] {
-    for (const ImexCtx* c : ens->members)
-      if (erosion_active(c)) return 1;
-    return 0;
-  }();
-  kb_step_begin<<<mgrid, 128, 0, st>>>(ens->dM, n, ens->n_active);
-  kb_mask<TS><<<(int)std::min<long long>(tiles, (long long)sms * 8), 256, 0, st>>>(
-      ens->dM, ens->tile_member, tiles, ens->active, ens->n_active);
-  kb_flux<NS, TS><<<(int)std::min<long long>(tiles, (long long)sms * flux_min_blocks<NS, TS>()),
-                    TS::THREADS, smem, st>>>(ens->dM, ens->tile_member, ens->active,
-                                             ens->n_active);
-  kb_dt_clip<<<mgrid, 128, 0, st>>>(ens->dM, n);
-  kb_stage2_first<NS><<<(int)std::min<long long>(tiles, (long long)sms * IMEX_FIRST_MINB),
-                        STAGE2_THREADS, 0, st>>>(ens->dM, ens->tile_member, ens->active,
-                                                 ens->n_active, tx, ty);
-  for (int pass = 0; pass < 3; ++pass) {
-    kb_list_offsets<<<1, 1024, 0, st>>>(ens->dM, n, pass, ens->list_off);
-    if (pass < 2)
-      kb_stage2_iter<NS><<<sms * IMEX_STAGE2_MINB, STAGE2_THREADS, 0, st>>>(ens->dM, n,
-                                                                              ens->list_off, pass + 2);
-    else
-      kb_stage2_tail<NS><<<sms * IMEX_STAGE2_MINB, STAGE2_THREADS, 0, st>>>(ens->dM, n,
-                                                                              ens->list_off);
-  }
-  kb_stage2_post<NS><<<(int)std::min<long long>(tiles, (long long)sms * 8), STAGE2_THREADS, 0,
-                       st>>>(ens->dM, ens->tile_member, ens->active, ens->n_active, tx, ty);
-  if (any_exchange)
-    kb_erosion<NS><<<(int)std::min<long long>(tiles, (long long)sms * IMEX_EROSION_MINB), 128, 0,
-                     st>>>(ens->dM, ens->tile_member, ens->active, ens->n_active, tx, ty);
-  kb_step_end<<<mgrid, 128, 0, st>>>(ens->dM, n);
-  ens->batch_launches = 13 + any_exchange;
-  return cudaGetLastError();
-}
-
-template <int NS>
-cudaError_t ens_enqueue_batch_shape(ImexEnsemble* ens, int si) {
-  switch (si) {
-    case 0: return ens_enqueue_batch_ns<NS, Shape32x8>(ens);
-    case 1: return ens_enqueue_batch_ns<NS, Shape16x16>(ens);
-    default: return ens_enqueue_batch_ns<NS, Shape32x4>(ens);
-  }
-}
-
+// One batched step of every member on ens->root (imex_batch.cu).
 cudaError_t ens_enqueue_batch(ImexEnsemble* ens, int si) {
-  switch (ens->members[0]->ns) {
-    case 1: return ens_enqueue_batch_shape<1>(ens, si);
-    case 2: return ens_enqueue_batch_shape<2>(ens, si);
-    case 3: return ens_enqueue_batch_shape<3>(ens, si);
-    default: return ens_enqueue_batch_shape<4>(ens, si);
-  }
+  imex_batch::Launch L{};
+  L.members = ens->dM;
+  L.n_members = (int)ens->members.size();
+  L.ns = ens->members[0]->ns;
+  L.shape = si;
+  L.tile_member = ens->tile_member;
+  L.active = ens->active;
+  L.n_active = ens->n_active;
+  L.list_off = ens->list_off;
+  L.n_tiles = ens->n_tiles;
+  L.any_exchange = 0;
+  for (const ImexCtx* c : ens->members)
+    if (erosion_active(c)) L.any_exchange = 1;
+  L.sms = sm_count(ens->device);
+  L.stream = ens->root;
+  int launches = 0;
+  cudaError_t e = imex_batch::enqueue_step(L, &launches);
+  ens->batch_launches = launches;
+  return e;
 }
 
 // Capture one batched step (tile shape si) into ens->graph.
@@ -1892,18 +1852,15 @@ int imex_gpu_ensemble_advance(ImexEnsemble* ens, int n_steps, int* first_bad_mem
   for (ImexCtx* c : ens->members) CKE(cudaStreamSynchronize(c->stream));
   const int nmem = (int)ens->members.size();
   int done = 0;
-  if (ens_batchable(ens)) {
-    // batched mode; tuning: one real step per candidate tile shape
+  const bool batched = ens->mode != 2 && ens_batchable(ens);
+  if (batched) {
+    // batched mode; tuning: real steps with the tile shapes in the order
+    // 0 1 2 2 1 0, so that a step cost that drifts linearly as the currents
+    // spread weighs on every shape alike; the smallest sum wins
     constexpr int n_shapes = (int)(sizeof(kShapes) / sizeof(kShapes[0]));
     while (ens->shape < 0 && done < n_steps) {
-      const int si = (int)ens->tried_shape.size();
-      if (si >= n_shapes) {
-        size_t best = 0;
-        for (size_t i = 1; i < ens->tried_shape_ms.size(); ++i)
-          if (ens->tried_shape_ms[i] < ens->tried_shape_ms[best]) best = i;
-        ens->shape = ens->tried_shape[best];
-        break;
-      }
+      const int k = (int)ens->tried_shape.size();
+      const int si = k < n_shapes ? k : 2 * n_shapes - 1 - k;
       int r = ens_build_batch_graph(ens, si);
       if (r) return r;
       float ms = 0.0f;
@@ -1912,14 +1869,17 @@ int imex_gpu_ensemble_advance(ImexEnsemble* ens, int n_steps, int* first_bad_mem
       ens->tried_shape.push_back(si);
       ens->tried_shape_ms.push_back(ms);
       ++done;
+      if ((int)ens->tried_shape.size() == 2 * n_shapes) {
+        double sum[n_shapes] = {0.0};
+        for (size_t i = 0; i < ens->tried_shape.size(); ++i)
+          sum[ens->tried_shape[i]] += ens->tried_shape_ms[i];
+        int best = 0;
+        for (int i = 1; i < n_shapes; ++i)
+          if (sum[i] < sum[best]) best = i;
+        ens->shape = best;
+      }
     }
-    if (done < n_steps && ens->shape < 0) {
-      // fewer steps than shapes: keep the best so far
-      size_t best = 0;
-      for (size_t i = 1; i < ens->tried_shape_ms.size(); ++i)
-        if (ens->tried_shape_ms[i] < ens->tried_shape_ms[best]) best = i;
-      ens->shape = ens->tried_shape[best];
-    }
+    if (done < n_steps && ens->shape < 0) ens->shape = ens->tried_shape.back();
     if (done < n_steps) {
       if (!ens->exec || ens->batch_shape != ens->shape || ens->graph_shape != ens->shape) {
         int r = ens_build_batch_graph(ens, ens->shape);
@@ -1932,7 +1892,7 @@ int imex_gpu_ensemble_advance(ImexEnsemble* ens, int n_steps, int* first_bad_mem
     }
   }
   // tuning: one real step per candidate stream count
-  while (!ens_batchable(ens) && ens->k_streams == 0 && done < n_steps) {
+  while (!batched && ens->k_streams == 0 && done < n_steps) {
     int k = ens->tried_k.empty() ? 1 : ens->tried_k.back() * 2;
     if (k > std::min(nmem, ENS_MAX_STREAMS)) {
       size_t best = 0;
@@ -1991,6 +1951,16 @@ int imex_gpu_ensemble_tuning(ImexEnsemble* ens, int* k_streams, int* n_tried, in
     ++n;
   }
   if (n_tried) *n_tried = n;
+  return IMEX_OK;
+}
+
+int imex_gpu_ensemble_set_mode(ImexEnsemble* ens, int mode) {
+  if (!ens || (mode != 0 && mode != 2)) return IMEX_EINVAL;
+  if (mode == ens->mode) return IMEX_OK;
+  CKE(cudaSetDevice(ens->device));
+  CKE(cudaStreamSynchronize(ens->root));
+  ens_drop_graph(ens);
+  ens->mode = mode;
   return IMEX_OK;
 }
 

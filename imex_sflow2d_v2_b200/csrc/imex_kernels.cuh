@@ -24,6 +24,7 @@
 #include "imex_mlp.cuh"
 
 namespace imex {
+inline namespace IMEX_TU_NS {
 
 constexpr int HALO = 2;
 
@@ -528,7 +529,7 @@ static_assert(Shape32x8::THREADS == 288, "k_flux blocks of 288 threads for 32x8 
 // Other tile shapes keep the register budget of three 288-thread blocks
 // (864 threads per SM) and fit as many blocks as shared memory allows.
 template <int NS, class TS = Shape32x8>
-constexpr int flux_min_blocks() {
+__host__ __device__ constexpr int flux_min_blocks() {
 #ifdef IMEX_FLUX_MINB
   return IMEX_FLUX_MINB;
 #else
@@ -2404,4 +2405,5 @@ __global__ void k_masks_xy(const __grid_constant__ DevParams Pp, const uint8_t* 
   }
 }
 
+}  // namespace IMEX_TU_NS
 }  // namespace imex

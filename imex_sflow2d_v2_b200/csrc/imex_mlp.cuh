@@ -20,6 +20,7 @@
 #include <cstdint>
 
 namespace imex {
+inline namespace IMEX_TU_NS {
 namespace mlp {
 
 constexpr int IN = 12, IN_P = 16;   // features (padded)
@@ -347,4 +348,5 @@ __global__ void k_gather_rows(const float* __restrict__ src, const long long* __
 }
 
 }  // namespace mlp
+}  // namespace IMEX_TU_NS
 }  // namespace imex

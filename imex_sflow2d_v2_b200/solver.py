@@ -112,6 +112,7 @@ def load_library(path=None, fast=False):
         "imex_gpu_ensemble_tuning": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int],
                                      C.c_int),
+        "imex_gpu_ensemble_set_mode": ([vp, C.c_int], C.c_int),
         "imex_gpu_ensemble_tile_shape": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                           C.POINTER(C.c_int), C.POINTER(C.c_int),
                                           C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int],
@@ -429,6 +430,13 @@ class ImexEnsemble:
         tm = (C.c_float * 16)()
         self.lib.imex_gpu_ensemble_tuning(self._h, C.byref(k), C.byref(n), tk, tm, 16)
         return k.value, [(tk[i], tm[i]) for i in range(min(n.value, 16))]
+
+    def set_mode(self, per_member_graphs=False):
+        """Per-member graphs over streams even when the members could be
+        batched (per_member_graphs=True), or batched when possible."""
+        rc = self.lib.imex_gpu_ensemble_set_mode(self._h, 2 if per_member_graphs else 0)
+        if rc != 0:
+            raise ImexError(rc, "imex_gpu_ensemble_set_mode")
 
     def tile_shape(self):
         """Batched mode: ((tx, ty) chosen, [((tx, ty), ms of its timed step),

@@ -352,10 +352,11 @@ int imex_gpu_harvest_data(ImexCtx* ctx, const float** x_dev, const float** y_dev
  * mask, the tiles holding a solve cell for the fluxes, stage 2 and erosion,
  * the members' Newton lists laid end to end for the iteration passes), 13
  * or 14 launches per step for the whole ensemble, captured once in a CUDA
- * graph and replayed.  Its first calls time one real step with each tile
- * shape of the mask and flux passes (32x8, 16x16, 32x4 cells) and keep the
- * fastest; imex_gpu_ensemble_tile_shape reports the chosen shape (0x0: not
- * batched) and the timed candidates.  Results equal each member's single
+ * graph and replayed.  Its first six steps are timed with the tile shapes
+ * of the mask and flux passes (32x8, 16x16, 32x4 cells) in the order
+ * 1 2 3 3 2 1, and the shape with the smallest total is kept;
+ * imex_gpu_ensemble_tile_shape reports the chosen shape (0x0: not batched or
+ * not tuned yet) and the timed steps.  Results equal each member's single
  * run bit for bit in both modes.
  */
 typedef struct ImexEnsemble ImexEnsemble;
@@ -366,6 +367,9 @@ int imex_gpu_ensemble_member(ImexEnsemble* ens, int m, ImexCtx** ctx);
 int imex_gpu_ensemble_advance(ImexEnsemble* ens, int n_steps, int* first_bad_member);
 int imex_gpu_ensemble_tuning(ImexEnsemble* ens, int* k_streams, int* n_tried, int* tried_k,
                              float* tried_ms, int cap);
+/* mode 0 (the default): batched when the members allow it; mode 2: always
+ * per-member graphs over streams.  Takes effect at the next advance. */
+int imex_gpu_ensemble_set_mode(ImexEnsemble* ens, int mode);
 int imex_gpu_ensemble_tile_shape(ImexEnsemble* ens, int* tx, int* ty, int* n_tried,
                                  int* tried_tx, int* tried_ty, float* tried_ms, int cap);
 const char* imex_gpu_ensemble_last_error(ImexEnsemble* ens);

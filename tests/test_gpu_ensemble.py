@@ -13,7 +13,7 @@ from imex_sflow2d_v2_b200.solver import ImexEnsemble, ImexSolver
 
 pytestmark = pytest.mark.gpu
 
-STEPS = 9   # more than the tuner's trial steps (3 tile shapes; 1, 2, 4 streams)
+STEPS = 9   # more than the tuner's trial steps (3 tile shapes twice; 1, 2, 4 streams)
 SHAPES = {(32, 8), (16, 16), (32, 4)}
 
 
@@ -65,7 +65,7 @@ def test_batched_ensemble_equals_single_runs():
     mem = _members()
     ens = _run(mem)
     shape, tried = ens.tile_shape()
-    assert shape in SHAPES and {s for s, ms in tried} == SHAPES
+    assert shape in SHAPES and {s for s, ms in tried} == SHAPES and len(tried) == 6
     assert all(ms > 0.0 for s, ms in tried)
     _check_against_single_runs(mem, ens)
     ens.close()
