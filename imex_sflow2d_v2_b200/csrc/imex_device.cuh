@@ -462,6 +462,64 @@ IMEX_QCQP_FN void qp_to_qc(const DevParams& P, const double* qp, double* qc) {
   for (int i = 0; i < NS; ++i) qc[4 + i] = xs[i] * qc[0];
 }
 
+// qp_to_qc and mixt_var of one face state in one pass: the volume fractions,
+// the carrier and the mixture densities, which both compute with the same
+// operations in the same order, are computed once (a state whose h is not
+// above EPS goes through mixt_var itself, so that NaN and dry states keep
+// both functions' own branches).
+template <int NS>
+IMEX_QCQP_FN void face_qc_mixt(const DevParams& P, const double* qp, double* qc, Mixt& m) {
+  constexpr int NV = 4 + NS;
+  double r_h = qp[0];
+  if (!(r_h > EPS)) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) qc[i] = 0.0;
+    m = mixt_var<NS>(P, qp);
+    return;
+  }
+  double r_hu = qp[1], r_hv = qp[2], r_u = qp[NV], r_v = qp[NV + 1], r_T = qp[3];
+  double al[NS], alr[NS];
+#pragma unroll
+  for (int i = 0; i < NS; ++i) al[i] = P.alpha_flag ? qp[4 + i] : qp[4 + i] / qp[0];
+  double at = 0.0;
+#pragma unroll
+  for (int i = 0; i < NS; ++i) at += al[i];
+#pragma unroll
+  for (int i = 0; i < NS; ++i) alr[i] = al[i] * P.rho_s[i];
+  double r_rho_a = P.pres / (P.sp_gas_const_a * r_T);
+  double r_rho_c = ((((1.0 - 0.0) - at) - 0.0) * r_rho_a + 0.0) / ((1.0 - 0.0) - at);
+  double r_alphac = 1.0 - at;
+  double sar = 0.0;
+#pragma unroll
+  for (int i = 0; i < NS; ++i) sar += alr[i];
+  double r_rho_m = r_alphac * r_rho_c + sar;
+  // mixt_var: rho_m = (1 - at)*rho_c + SUM(al*rho_s), the same operations
+  m.rho_c = r_rho_c;
+  m.rho_m = r_rho_m;
+  m.red_grav = (r_rho_m - P.rho_a_amb) / r_rho_m * P.grav;
+  const double vel2 = r_u * r_u + r_v * r_v;
+  m.Ri = (vel2 > 0.0) ? fmin_f(1.0e15, m.red_grav * r_h / vel2) : 0.0;
+  double r_inv_rhom = 1.0 / r_rho_m;
+  double xs[NS];
+#pragma unroll
+  for (int i = 0; i < NS; ++i) xs[i] = alr[i] * r_inv_rhom;
+  double r_xc = r_alphac * r_rho_c * r_inv_rhom;
+  double cpc = (r_xc > EPS) ? ((r_xc - 0.0) * P.sp_heat_a + 0.0) / r_xc : P.sp_heat_a;
+  double dot = 0.0;
+#pragma unroll
+  for (int i = 0; i < NS; ++i) dot += xs[i] * P.sp_heat_s[i];
+  double cpm = dot + r_xc * cpc;
+  qc[0] = r_rho_m * r_h;
+  qc[1] = r_rho_m * r_hu;
+  qc[2] = r_rho_m * r_hv;
+  if (P.energy_flag)
+    qc[3] = (r_h > 0.0) ? r_h * r_rho_m * (cpm * r_T + 0.5 * (r_u * r_u + r_v * r_v)) : 0.0;
+  else
+    qc[3] = r_h * r_rho_m * cpm * r_T;
+#pragma unroll
+  for (int i = 0; i < NS; ++i) qc[4 + i] = xs[i] * qc[0];
+}
+
 // ----------------------------------------------------------- limiters
 IMEX_HD double minmod(double a, double b) {
   if (fmin_f(fabs(a), fabs(b)) <= 0.0) return 0.0;

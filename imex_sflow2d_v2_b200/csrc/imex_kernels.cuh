@@ -55,10 +55,10 @@ constexpr int NYI = Shape32x8::NYI;
 
 // Minimum resident blocks per SM asked of ptxas for the flux and per-cell
 // kernels (their register budget); tuning knobs, set with -D at build time.
-// The Newton list passes run at 80 registers (6 blocks of 128): 10.0 ms per
-// step at 4096^2 against 10.3 at 64 and 72 registers.
+// The Newton list passes run at 96 registers (5 blocks of 128): 9.8 ms per
+// step at 4096^2 against 9.9 at 80 registers and 10.3 at 64 and 72.
 #ifndef IMEX_STAGE2_MINB
-#define IMEX_STAGE2_MINB 6
+#define IMEX_STAGE2_MINB 5
 #endif
 #ifndef IMEX_EROSION_MINB
 #define IMEX_EROSION_MINB 8
@@ -447,9 +447,9 @@ IMEX_FLAT void interface_flux(const DevParams& P, const Tile<NS, TS>& T, int dir
     }
   }
   double cL[NV], cR[NV];
-  qp_to_qc<NS>(P, QL, cL);
-  qp_to_qc<NS>(P, QR, cR);
-  Mixt mL = mixt_var<NS>(P, QL), mR = mixt_var<NS>(P, QR);
+  Mixt mL, mR;
+  face_qc_mixt<NS>(P, QL, cL, mL);
+  face_qc_mixt<NS>(P, QR, cR, mR);
   double lmin, lmax, rmin, rmax;
   local_speeds<NS>(P, QL, mL, gcf, dir, lmin, lmax);
   local_speeds<NS>(P, QR, mR, gcf, dir, rmin, rmax);
@@ -805,7 +805,7 @@ IMEX_EVAL_FN void eval_f(const DevParams& P, const double* qj, const double* qj_
 // Jacobian columns 2,3 by complex step (src/solver_2d.f90:2300-2365) and the
 // Newton direction: explicit rows diagonal, 2x2 Cramer on rows/cols 2,3
 // (src/solver_2d.f90:1879-1901).
-template <int NS>
+template <int NS, bool COLS_TOGETHER = false>
 IMEX_FLAT void newton_direction(const DevParams& P, double bx, double by, double dt,
                                               const double* qj_org, const double* qj_rel,
                                               const double* rt, double* dd, double* J2,
@@ -818,8 +818,7 @@ IMEX_FLAT void newton_direction(const DevParams& P, double bx, double by, double
     for (int m = 0; m < NV; ++m) qc[m] = mulr(C(qj_rel[m], 0.0), qj_org[m]);
     implicit_prefix_c<NS>(P, qc, pre);
   }
-#pragma unroll 1
-  for (int col = 1; col <= 2; ++col) {
+  auto column = [&](int col) {
     cplx qc[NV];
 #pragma unroll
     for (int m = 0; m < NV; ++m) qc[m] = mulr(C(qj_rel[m], (m == col) ? P.hstep : 0.0), qj_org[m]);
@@ -834,6 +833,15 @@ IMEX_FLAT void newton_direction(const DevParams& P, double bx, double by, double
       if (col == 1) J2[r] = v;
       else J3[r] = v;
     }
+  };
+  // the two columns one after the other, or (COLS_TOGETHER) unrolled, so
+  // that the scheduler may interleave their independent chains
+  if constexpr (COLS_TOGETHER) {
+#pragma unroll
+    for (int col = 1; col <= 2; ++col) column(col);
+  } else {
+#pragma unroll 1
+    for (int col = 1; col <= 2; ++col) column(col);
   }
   double d1[NV];
 #pragma unroll
@@ -966,7 +974,9 @@ IMEX_FLAT bool newton_iterk(const DevParams& P, double* qj, const double* qj_old
     if (newton_restart<NS>(P, qj, qj_old, Rj, bx, by, dt, qj_org, qj_rel, rt, scal_f)) return true;
   }
   double dd[NV], J2[NV], J3[NV], x_old[NV];
-  newton_direction<NS>(P, bx, by, dt, qj_org, qj_rel, rt, dd, J2, J3);
+  // the later iterations evaluate the Jacobian columns side by side (0.3 ms
+  // per step less at 4096^2 than one column at a time)
+  newton_direction<NS, true>(P, bx, by, dt, qj_org, qj_rel, rt, dd, J2, J3);
 #pragma unroll
   for (int i = 0; i < NV; ++i) x_old[i] = qj_rel[i];
   const double scal_f_old = scal_f;
