@@ -156,7 +156,13 @@ IMEX_HD void two_prod(double a, double b, double& p, double& e) {
   p = a * b;
   e = fma(a, b, -p);
 }
-IMEX_IPOW_FN double ipow(double x, double y) {
+// The body, inlined where one call site runs in a loop (the settling drag);
+// `ipow` below is the called copy.  Two library calls are replaced by exact
+// bit operations on their common ranges: frexp of a positive normal x (the
+// exponent field and the fraction with the exponent of [1, 2)), and ldexp
+// by a power of two whose product stays normal (an exact product).  The top
+// seven fraction bits are (m - 1)*128 truncated, read from the bits.
+IMEX_HD double ipow_body(double x, double y) {
   if (isnan(x) || isnan(y)) return x + y;
   if (x == 0.0 && y != 0.0) return (y > 0.0) ? 0.0 : __longlong_as_double(0x7ff0000000000000LL);
   if (x < 0.0 && y != 0.0) return __longlong_as_double(0x7ff8000000000000LL);
@@ -167,11 +173,21 @@ IMEX_IPOW_FN double ipow(double x, double y) {
   const double LN2_64_HI = 0x1.62e42fee00000p-7, LN2_64_LO = 0x1.a39ef35793c76p-39;
   const double INV_LN2_64 = 0x1.71547652b82fep+6;
   // log x = e*ln2 - log(invc_i) + log1p(r), m*invc_i = 1 + r, |r| < 2^-8
-  int e;
-  double m = frexp(x, &e);          // m in [1/2, 1)
-  m = m * 2.0;
-  e = e - 1;
-  const int i = (int)((m - 1.0) * 128.0);
+  int e, i;
+  double m;
+  const long long xb = __double_as_longlong(x);
+  const int ef = (int)(xb >> 52);   // x > 0 here: the sign bit is clear
+  if (ef > 0) {
+    // normal: m = x with the exponent of [1, 2), e the unbiased exponent
+    m = __longlong_as_double((xb & 0x000fffffffffffffLL) | 0x3ff0000000000000LL);
+    e = ef - 1023;
+    i = (int)((xb >> 45) & 127);
+  } else {
+    m = frexp(x, &e);               // m in [1/2, 1)
+    m = m * 2.0;
+    e = e - 1;
+    i = (int)((m - 1.0) * 128.0);
+  }
   const double r = fma(m, IPOW_INVC[i], -1.0);
   double P = fma(r, 0x1.2492492492492p-3, -0x1.5555555555555p-3);   // 1/7, -1/6
   P = fma(r, P, 0x1.999999999999ap-3);                               // 1/5
@@ -205,8 +221,12 @@ IMEX_IPOW_FN double ipow(double x, double y) {
   E = fma(rr, E, 0x1.0000000000000p-1);                              // 1/2
   const double em1 = fma(rr * rr, E, rr);
   const double th = IPOW_EXP2_HI[j];
-  return ldexp(th + fma(th, em1, IPOW_EXP2_LO[j]), me);
+  const double v = th + fma(th, em1, IPOW_EXP2_LO[j]);   // in [1, 2]
+  if (me >= -1000 && me <= 1000)
+    return v * __longlong_as_double((long long)(me + 1023) << 52);
+  return ldexp(v, me);
 }
+IMEX_IPOW_FN double ipow(double x, double y) { return ipow_body(x, y); }
 
 // ------------------------------------------------------------- complex
 struct cplx {
@@ -521,26 +541,51 @@ IMEX_QCQP_FN void face_qc_mixt(const DevParams& P, const double* qp, double* qc,
 }
 
 // ----------------------------------------------------------- limiters
+// minmod/maxmod (src/geometry_2d.f90:1555-1676).  The signs a/|a|, b/|b| of
+// finite nonzero operands are exactly +-1, so 0.5*(sa + sb) is exactly +-1
+// (same signs) or +0 (opposite signs, 1 + -1 = +0): the result is then
+// +-min (+-max) or +0 without the two divisions.  Infinite or NaN operands
+// take the reference's expression.
 IMEX_HD double minmod(double a, double b) {
   if (fmin_f(fabs(a), fabs(b)) <= 0.0) return 0.0;
+  if (isfinite(a) && isfinite(b)) {
+    const double m = fmin_f(fabs(a), fabs(b));
+    return ((a > 0.0) == (b > 0.0)) ? ((a > 0.0) ? m : -m) : 0.0;
+  }
   double sa = a / fabs(a), sb = b / fabs(b);
   return 0.5 * (sa + sb) * fmin_f(fabs(a), fabs(b));
 }
 IMEX_HD double maxmod(double a, double b) {
   if (fabs(a * b) <= 0.0) return 0.0;
+  if (isfinite(a) && isfinite(b)) {
+    const double m = fmax_f(fabs(a), fabs(b));
+    return ((a > 0.0) == (b > 0.0)) ? ((a > 0.0) ? m : -m) : 0.0;
+  }
   double sa = a / fabs(a), sb = b / fabs(b);
   return 0.5 * (sa + sb) * fmax_f(fabs(a), fabs(b));
 }
+// limit() with limiter 1 (minmod) on equally spaced centres, z3 - z2 ==
+// z2 - z1 == dz > 0.  For finite differences d3, d1 of one sign the two
+// slopes are d3/dz and d1/dz; rounded division by a positive dz is monotone,
+// so the smaller slope magnitude is the rounded quotient of the smaller
+// difference: one division instead of two.  Where a quotient could overflow
+// (an infinite slope makes minmod NaN) or a difference is not finite,
+// limit() itself is used.
+IMEX_HD double minmod_uniform(double v1, double v2, double v3, double dz, double z1, double z2,
+                              double z3, double theta);
 IMEX_LIMIT_FN double limit(double v1, double v2, double v3, double z1, double z2, double z3,
                         int lim, double theta) {
   if (lim == 1) {
     // minmod(a,b) with a=(v3-v2)/(z3-z2), b=(v2-v1)/(z2-z1), z increasing:
-    // when the two differences are finite and of opposite sign (or one is
-    // zero) the result is exactly 0 and the quotients are not needed.
+    // when one difference is zero, or the two are finite, of opposite sign
+    // and their quotients cannot overflow (an infinite quotient makes
+    // minmod NaN), the result is exactly 0 and the quotients are not needed.
     double d3 = v3 - v2, d1 = v2 - v1;
     if (isfinite(d3) && isfinite(d1) && (z3 > z2) && (z2 > z1)) {
       if (d3 == 0.0 || d1 == 0.0) return 0.0;
-      if ((d3 > 0.0) != (d1 > 0.0)) return 0.0;
+      if ((d3 > 0.0) != (d1 > 0.0) && fmax_f(fabs(d3), fabs(d1)) <= 1e290 &&
+          z3 - z2 >= 1e-10 && z2 - z1 >= 1e-10)
+        return 0.0;
     }
     double a = d3 / (z3 - z2);
     double b = d1 / (z2 - z1);
@@ -559,6 +604,21 @@ IMEX_LIMIT_FN double limit(double v1, double v2, double v3, double z1, double z2
     case 7: return b;
   }
   return 0.0;
+}
+IMEX_HD double minmod_uniform(double v1, double v2, double v3, double dz, double z1, double z2,
+                              double z3, double theta) {
+  const double d3 = v3 - v2, d1 = v2 - v1;
+  if (isfinite(d3) && isfinite(d1)) {
+    if (d3 == 0.0 || d1 == 0.0) return 0.0;
+    const double a3 = fabs(d3), a1 = fabs(d1);
+    if (fmax_f(a3, a1) <= 1e290 && dz >= 1e-10) {
+      if ((d3 > 0.0) != (d1 > 0.0)) return 0.0;
+      const double q = fmin_f(a3, a1) / dz;
+      if (q <= 0.0) return 0.0;
+      return (d3 > 0.0) ? q : -q;
+    }
+  }
+  return limit(v1, v2, v3, z1, z2, z3, 1, theta);
 }
 
 // ------------------------------------------------------ source boundary
@@ -911,6 +971,22 @@ IMEX_HD void semi_impl_terms(const DevParams& P, double bx, double by, double bx
 }
 
 // ------------------------------------------------------ mass exchange
+// (d / s < t) for the rounded quotient, without the division where the
+// answer is certain.  With s and t positive and s*t normal, the products
+// below are within 2^-52 relative of s*t*(1 -+ 2^-40): below the lower one,
+// d/s < t*(1 - 2^-41), whose rounding is already below t (t's half ulp is
+// t*2^-53); above the upper one, d/s > t*(1 + 2^-41) rounds above t.
+// Rounding is monotone, so the quotient compares as the bounds do.  Between
+// them, and outside the ranges, the quotient is taken.
+IMEX_HD bool rel_change_below(double d, double s, double t) {
+  if (s > 1e-200 && s < 1e200 && d <= 1e300) {
+    const double st = s * t;
+    if (d < st * (1.0 - 0x1p-40)) return true;
+    if (d > st * (1.0 + 0x1p-40)) return false;
+  }
+  return d / s < t;
+}
+
 IMEX_SETTLE_FN double settling_velocity(const DevParams& P, double diam, double rhos, double rhoc,
                                  double ikv) {
   double inv_sqrt_C_D = 1.0;
@@ -921,9 +997,9 @@ IMEX_SETTLE_FN double settling_velocity(const DevParams& P, double diam, double 
   if (Rey <= 1000.0) {
     for (int i = 1; i <= 20; ++i) {
       double sv_old = sv;
-      inv_sqrt_C_D = sqrt(Rey / (24.0 * (1.0 + 0.15 * ipow(Rey, 0.687))));
+      inv_sqrt_C_D = sqrt(Rey / (24.0 * (1.0 + 0.15 * ipow_body(Rey, 0.687))));
       sv = const_part * inv_sqrt_C_D;
-      if (fabs(sv_old - sv) / sv_old < 1.0e-6) return sv;
+      if (rel_change_below(fabs(sv_old - sv), sv_old, 1.0e-6)) return sv;
       Rey = diam * sv * ikv;
     }
   }

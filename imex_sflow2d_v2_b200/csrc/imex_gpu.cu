@@ -412,8 +412,48 @@ int validate(const ImexParams* p, std::string& why) {
 
 }  // namespace
 
+namespace {
+__global__ void k_point_eval(int fn, long long n, const double* __restrict__ a,
+                             const double* __restrict__ b, const double* __restrict__ c,
+                             const double* __restrict__ d, double g, double* __restrict__ out) {
+  DevParams P;
+  P.grav = g;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = (fn == 0)   ? ipow(a[i], b[i])
+             : (fn == 1) ? settling_velocity(P, a[i], b[i], c[i], d[i])
+             : (fn == 2) ? minmod_uniform(a[i], b[i], c[i], d[i], 0.0, d[i], 2.0 * d[i], 1.0)
+                         : limit(a[i], b[i], c[i], 0.0, d[i], 2.0 * d[i], (int)g, 1.0);
+}
+}  // namespace
+
 // ====================================================================== ABI
 extern "C" {
+
+int imex_gpu_point_eval(int fn, long long n, const double* a, const double* b, const double* c,
+                        const double* d, double g, double* out) {
+  if (fn < 0 || fn > 3 || n < 0 || !a || !b || !out || (fn >= 1 && (!c || !d)))
+    return IMEX_EINVAL;
+  if (n == 0) return IMEX_OK;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return IMEX_ENODEVICE;
+  const size_t bytes = (size_t)n * sizeof(double);
+  double* buf = nullptr;
+  if (cudaMalloc(&buf, 5 * bytes) != cudaSuccess) return IMEX_ENOMEM;
+  double *da = buf, *db = buf + n, *dc = buf + 2 * n, *dd = buf + 3 * n, *dout = buf + 4 * n;
+  cudaError_t e = cudaMemcpy(da, a, bytes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(db, b, bytes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && fn >= 1) e = cudaMemcpy(dc, c, bytes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && fn >= 1) e = cudaMemcpy(dd, d, bytes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    const int grid = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+    k_point_eval<<<grid, 256>>>(fn, n, da, db, dc, dd, g, dout);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, dout, bytes, cudaMemcpyDeviceToHost);
+  cudaFree(buf);
+  return e == cudaSuccess ? IMEX_OK : IMEX_ECUDA;
+}
 
 const char* imex_gpu_build_info(void) {
 #ifdef IMEX_FMAD

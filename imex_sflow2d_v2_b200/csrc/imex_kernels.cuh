@@ -370,11 +370,16 @@ __device__ __forceinline__ void precompute_slopes(const DevParams& P, const Tile
         const double z1 = (dir == 1) ? x_comp(P, I - 1) : y_comp(P, I - 1);
         const double z2 = (dir == 1) ? x_comp(P, I) : y_comp(P, I);
         const double z3 = (dir == 1) ? x_comp(P, I + 1) : y_comp(P, I + 1);
+        const double dz = z3 - z2;
+        const bool uniform = (dz == z2 - z1) && (z3 > z2) && (z2 > z1);
 #pragma unroll 1
         for (int i = 0; i < NP; ++i) {
           const double v1 = T.qp[i][ly - dy_][lx - dx_], v2 = T.qp[i][ly][lx],
                        v3 = T.qp[i][ly + dy_][lx + dx_];
-          D.dq[i][ly - 1][lx - 1] = rc_d * limit(v1, v2, v3, z1, z2, z3, P.limiter[i], P.theta);
+          const double lim = (uniform && P.limiter[i] == 1)
+                                 ? minmod_uniform(v1, v2, v3, dz, z1, z2, z3, P.theta)
+                                 : limit(v1, v2, v3, z1, z2, z3, P.limiter[i], P.theta);
+          D.dq[i][ly - 1][lx - 1] = rc_d * lim;
         }
         ok = 1;
       }

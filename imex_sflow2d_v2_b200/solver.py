@@ -71,6 +71,8 @@ def load_library(path=None, fast=False):
         "imex_gpu_kernel_times": ([vp, dp, i64p, C.c_int], C.c_int),
         "imex_gpu_measure_fp64_peak": ([C.c_int, dp], C.c_int),
         "imex_gpu_build_info": ([], C.c_char_p),
+        "imex_gpu_point_eval": ([C.c_int, C.c_longlong, dp, dp, dp, dp, C.c_double, dp],
+                                C.c_int),
         "imex_setup_dem": ([C.c_int, C.c_int, C.c_int] + [C.c_double] * 4 + [dp, C.c_int, C.c_int]
                            + [C.c_double] * 3 + [dp, i8p, C.POINTER(C.c_float)], C.c_int),
         "imex_setup_cell_fract": ([C.c_int, C.c_int, C.c_int] + [C.c_double] * 8
@@ -551,3 +553,24 @@ def format_edit(kind, value, w, d=0, e=0):
     if n < 0:
         raise ValueError("imex_format_edit: bad arguments")
     return buf.value.decode()
+
+
+def point_eval(fn, a, b, c=None, d=None, g=0.0, fast=False):
+    """The device's point functions on host arrays (imex_gpu_point_eval):
+    fn "ipow" gives a**b, fn "settling" settling_velocity(a, b, c, d) with
+    gravity g, "minmod_uniform" the minmod slope of a, b, c at centres 0, d,
+    2d by the flux kernel's equal-spacing path, "limit" limit() at those
+    centres with limiter g.  Arrays are broadcast to one shape."""
+    code = {"ipow": 0, "settling": 1, "minmod_uniform": 2, "limit": 3}[fn]
+    arrs = [np.ascontiguousarray(x, dtype=np.float64)
+            for x in np.broadcast_arrays(a, b, *(() if code == 0 else (c, d)))]
+    while len(arrs) < 4:
+        arrs.append(arrs[0])
+    out = np.empty(arrs[0].shape)
+    L = load_library(fast=fast)
+    p = [x.ctypes.data_as(C.POINTER(C.c_double)) for x in arrs]
+    rc = L.imex_gpu_point_eval(code, out.size, *p, float(g),
+                               out.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc != 0:
+        raise ImexError(rc, "point_eval")
+    return out

@@ -461,6 +461,21 @@ int imex_setup_regrid(int device, int ncols, int nrows, double xllcorner, double
                       double x0, double y0, double cell_size, double* fout, float* kernel_ms);
 const char* imex_setup_last_error(void);
 
+/* Point functions of the step evaluated on the device, element by element,
+ * for host arrays of n values (copied in, evaluated, copied out); a check of
+ * the CUDA point functions against another implementation on any inputs.
+ *   fn 0  x**y, the table-driven power of the mass-exchange closures:
+ *         out = a**b (c, d unused)
+ *   fn 1  settling_velocity(diam = a, rhos = b, rhoc = c, 1/kin_visc = d)
+ *         with gravity g          src/constitutive_2d.f90:5148-5214
+ *   fn 2  the limiter-1 (minmod) slope of values a, b, c at centres 0, d, 2d
+ *         by the equal-spacing path of the flux kernel
+ *   fn 3  limit(a, b, c at centres 0, d, 2d) with limiter g (0..7), theta 1
+ *         src/geometry_2d.f90:1555-1676
+ * Returns IMEX_EINVAL for another fn or n < 0, IMEX_ENODEVICE without a GPU. */
+int imex_gpu_point_eval(int fn, long long n, const double* a, const double* b, const double* c,
+                        const double* d, double g, double* out);
+
 /* Build information: "sm_100a fmad=0 ..." */
 const char* imex_gpu_build_info(void);
 

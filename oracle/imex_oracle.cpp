@@ -772,11 +772,11 @@ void OracleCtx::eval_nh_semi_impl_terms(double bx, double by, double bxx, double
 }
 
 // src/constitutive_2d.f90:5148-5214
-double OracleCtx::settling_velocity(double diam, double rhos, double rhoc,
-                                    double ikv) const {
+static double settling_velocity_g(double diam, double rhos, double rhoc, double ikv,
+                                  double grav) {
   double inv_sqrt_C_D = 1.0;
   if (rhos <= rhoc) return 0.0;
-  double const_part = std::sqrt(0.75 * (rhos / rhoc - 1.0) * diam * p.grav);
+  double const_part = std::sqrt(0.75 * (rhos / rhoc - 1.0) * diam * grav);
   double sv = const_part * inv_sqrt_C_D;
   double Rey = diam * sv * ikv;
   if (Rey <= 1000.0) {
@@ -789,6 +789,10 @@ double OracleCtx::settling_velocity(double diam, double rhos, double rhoc,
     }
   }
   return sv;
+}
+double OracleCtx::settling_velocity(double diam, double rhos, double rhoc,
+                                    double ikv) const {
+  return settling_velocity_g(diam, rhos, rhoc, ikv, p.grav);
 }
 
 // src/constitutive_2d.f90:4424-5003 (no liquid, no pore pressure, no profiles)
@@ -2615,6 +2619,28 @@ int oracle_solve_rk_step(OracleCtx* o, double* qj, const double* qj_old,
 }
 
 double oracle_ipow(double x, double y) { return ipow(x, y); }
+void oracle_ipow_n(long long n, const double* x, const double* y, double* out) {
+#pragma omp parallel for schedule(static)
+  for (long long i = 0; i < n; ++i) out[i] = ipow(x[i], y[i]);
+}
+void oracle_limit_n(long long n, const double* v1, const double* v2, const double* v3,
+                    const double* z1, const double* z2, const double* z3, int limiter,
+                    double theta, double* out) {
+  OracleCtx tmp;
+  tmp.p.theta = theta;
+#pragma omp parallel for schedule(static)
+  for (long long i = 0; i < n; ++i) {
+    const double v[3] = {v1[i], v2[i], v3[i]}, z[3] = {z1[i], z2[i], z3[i]};
+    out[i] = tmp.limit(v, z, limiter);
+  }
+}
+void oracle_settling_velocity_n(long long n, const double* diam, const double* rhos,
+                                const double* rhoc, const double* ikv, double grav,
+                                double* out) {
+#pragma omp parallel for schedule(static)
+  for (long long i = 0; i < n; ++i)
+    out[i] = settling_velocity_g(diam[i], rhos[i], rhoc[i], ikv[i], grav);
+}
 
 double oracle_limit(double v1, double v2, double v3, double z1, double z2, double z3,
                     int limiter, double theta) {

@@ -82,6 +82,14 @@ void oracle_eval_fluxes(OracleCtx* o, const double* qc, const double* qp, double
 void oracle_kt_interface(OracleCtx* o, const double* qcL, const double* qpL, const double* qcR,
                          const double* qpR, double gcf, int dir, double* H, double* speeds);
 double oracle_ipow(double x, double y);
+// element-wise over n values (OpenMP): x**y, and settling_velocity with gravity grav
+void oracle_ipow_n(long long n, const double* x, const double* y, double* out);
+void oracle_limit_n(long long n, const double* v1, const double* v2, const double* v3,
+                    const double* z1, const double* z2, const double* z3, int limiter,
+                    double theta, double* out);
+void oracle_settling_velocity_n(long long n, const double* diam, const double* rhos,
+                                const double* rhoc, const double* ikv, double grav,
+                                double* out);
 double oracle_limit(double v1, double v2, double v3, double z1, double z2,
                     double z3, int limiter, double theta);
 

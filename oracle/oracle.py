@@ -89,6 +89,9 @@ def lib(target=CHECKER):
                                            C.c_double, C.c_double]
         L.oracle_ipow.restype = C.c_double
         L.oracle_ipow.argtypes = [C.c_double, C.c_double]
+        L.oracle_ipow_n.argtypes = [C.c_longlong, dp, dp, dp]
+        L.oracle_settling_velocity_n.argtypes = [C.c_longlong, dp, dp, dp, dp, C.c_double, dp]
+        L.oracle_limit_n.argtypes = [C.c_longlong] + [dp] * 6 + [C.c_int, C.c_double, dp]
         L.oracle_post_init.argtypes = [vp, C.c_int, dp, C.c_int, dp]
         L.oracle_post_diag.argtypes = [vp, dp]
         L.oracle_get_post.argtypes = [vp, dp, dp, dp, C.POINTER(C.c_int8)]
@@ -313,6 +316,33 @@ class Oracle:
 
 def ipow(x, y):
     return lib().oracle_ipow(float(x), float(y))
+
+
+def ipow_n(x, y):
+    """x**y element by element (arrays of one shape)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(np.broadcast_to(y, x.shape), dtype=np.float64)
+    out = np.empty_like(x)
+    lib().oracle_ipow_n(x.size, _p(x), _p(y), _p(out))
+    return out
+
+
+def limit_n(v1, v2, v3, z1, z2, z3, limiter, theta=1.0):
+    """limit() element by element (arrays broadcast to one shape)."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float64)
+            for a in np.broadcast_arrays(v1, v2, v3, z1, z2, z3)]
+    out = np.empty(arrs[0].shape)
+    lib().oracle_limit_n(out.size, *[_p(a) for a in arrs], int(limiter), float(theta), _p(out))
+    return out
+
+
+def settling_velocity_n(diam, rhos, rhoc, ikv, grav):
+    """settling_velocity element by element (arrays broadcast to one shape)."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float64)
+            for a in np.broadcast_arrays(diam, rhos, rhoc, ikv)]
+    out = np.empty(arrs[0].shape)
+    lib().oracle_settling_velocity_n(out.size, *[_p(a) for a in arrs], float(grav), _p(out))
+    return out
 
 
 def limit(v1, v2, v3, z1, z2, z3, limiter, theta=1.0):
