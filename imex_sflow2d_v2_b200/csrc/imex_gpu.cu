@@ -423,7 +423,8 @@ __global__ void k_point_eval(int fn, long long n, const double* __restrict__ a,
     out[i] = (fn == 0)   ? ipow(a[i], b[i])
              : (fn == 1) ? settling_velocity(P, a[i], b[i], c[i], d[i])
              : (fn == 2) ? minmod_uniform(a[i], b[i], c[i], d[i], 0.0, d[i], 2.0 * d[i], 1.0)
-                         : limit(a[i], b[i], c[i], 0.0, d[i], 2.0 * d[i], (int)g, 1.0);
+             : (fn == 3) ? limit(a[i], b[i], c[i], 0.0, d[i], 2.0 * d[i], (int)g, 1.0)
+                         : (rel_change_below(a[i], b[i], c[i]) ? 1.0 : 0.0);
 }
 }  // namespace
 
@@ -432,7 +433,7 @@ extern "C" {
 
 int imex_gpu_point_eval(int fn, long long n, const double* a, const double* b, const double* c,
                         const double* d, double g, double* out) {
-  if (fn < 0 || fn > 3 || n < 0 || !a || !b || !out || (fn >= 1 && (!c || !d)))
+  if (fn < 0 || fn > 4 || n < 0 || !a || !b || !out || (fn >= 1 && (!c || !d)))
     return IMEX_EINVAL;
   if (n == 0) return IMEX_OK;
   int ndev = 0;

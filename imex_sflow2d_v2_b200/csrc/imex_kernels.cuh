@@ -884,13 +884,20 @@ __device__ __forceinline__ bool newton_converged(const double* rt, const double*
 #pragma unroll
   for (int i = 1; i < NV; ++i) mx = fmax_f(mx, fabs(rt[i]));
   if (mx < NEWTON_TOLF) return true;
-  double m3 = 0.0;
+  // m3 = MAX over i of |qj_rel - x_old| / MAX(|qj_rel|, 1) < EPS.  MAX skips
+  // NaN quotients (all NaN: NaN, and the test fails), so the test holds when
+  // some quotient is a number and every such quotient is below EPS; each
+  // comparison of a rounded quotient is taken without the division where
+  // its answer is certain (rel_change_below).
+  bool any = false, below = true;
 #pragma unroll
   for (int i = 0; i < NV; ++i) {
-    double r = fabs(qj_rel[i] - x_old[i]) / fmax_f(fabs(qj_rel[i]), 1.0);
-    m3 = (i == 0) ? r : fmax_f(m3, r);
+    const double d = fabs(qj_rel[i] - x_old[i]), s = fmax_f(fabs(qj_rel[i]), 1.0);
+    if (isnan(d) || (isinf(d) && isinf(s))) continue;   // the quotient is NaN
+    any = true;
+    below = below & rel_change_below(d, s, EPS);
   }
-  return m3 < EPS;
+  return any && below;
 }
 
 // Scaling (src/solver_2d.f90:1786-1798); the residual test before the first
@@ -1003,25 +1010,36 @@ IMEX_FLAT bool newton_iterk(const DevParams& P, double* qj, const double* qj_old
     }
     grad[c] = s;
   }
-  double scale = 0.0, ssq = 0.0;
+  // NORM2(dd) > stpmax scales the step.  The scaled sum below ends with
+  // scale = MAX|dd| and ssq <= NV (each term at most 1) up to a few
+  // roundings, so its result is below 3*MAX|dd| for NV <= 8; when that bound
+  // is already below stpmax (finite), the norm cannot exceed it and is not
+  // evaluated.  A NaN component gives a NaN norm and no scaling either way.
+  static_assert(NV <= 8, "the norm bound 3*MAX|dd| holds for up to 8 components");
+  double dmax = 0.0;
 #pragma unroll
-  for (int i = 0; i < NV; ++i) {
-    if (dd[i] != 0.0) {
-      double ax = fabs(dd[i]);
-      if (scale < ax) {
-        double val = scale / ax;
-        ssq = 1.0 + ssq * val * val;
-        scale = ax;
-      } else {
-        double val = ax / scale;
-        ssq = ssq + val * val;
+  for (int i = 0; i < NV; ++i) dmax = fmax_f(dmax, fabs(dd[i]));
+  if (!(3.0 * dmax < stpmax)) {
+    double scale = 0.0, ssq = 0.0;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      if (dd[i] != 0.0) {
+        double ax = fabs(dd[i]);
+        if (scale < ax) {
+          double val = scale / ax;
+          ssq = 1.0 + ssq * val * val;
+          scale = ax;
+        } else {
+          double val = ax / scale;
+          ssq = ssq + val * val;
+        }
       }
     }
-  }
-  double dabs = scale * sqrt(ssq);
-  if (dabs > stpmax) {
+    double dabs = scale * sqrt(ssq);
+    if (dabs > stpmax) {
 #pragma unroll
-    for (int i = 0; i < NV; ++i) dd[i] = dd[i] * stpmax / dabs;
+      for (int i = 0; i < NV; ++i) dd[i] = dd[i] * stpmax / dabs;
+    }
   }
   double slope = 0.0;
 #pragma unroll
@@ -1040,44 +1058,79 @@ IMEX_FLAT bool newton_iterk(const DevParams& P, double* qj, const double* qj_old
 #pragma unroll
     for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i];
   } else {
+    // Rows other than 2, 3 carry no implicit term: eval_f's sum of f^2
+    // taken over them alone, in eval_f's order, cannot exceed the full sum
+    // (rounded addition of a term >= 0 never decreases a sum, and rounding
+    // is monotone).  When that partial half-sum already exceeds
+    // 0.9*scal_f_old the trial fails whatever the implicit terms are, and
+    // the implicit terms are not evaluated.  Only for trials whose failure
+    // is all that matters: not trial 0 and not alam = 1 (their scal_f sets
+    // the next alam), and with a finite old iterate (then the residual left
+    // by the last trial is never read: a search that puts the old iterate
+    // back ends the iteration as converged).
+    //
+    // After the first backtrack every alam is half the previous one,
+    // whatever a trial's outcome, so two consecutive trials' partial sums
+    // are evaluated side by side (independent chains) and their outcomes
+    // then taken in order, as one trial after the other.
+    auto partial_half_sum = [&](double al) {
+      double d = 0.0;
+#pragma unroll
+      for (int i = 0; i < NV; ++i) {
+        if (i == 1 || i == 2) continue;
+        const double qt = (x_old[i] + al * dd[i]) * qj_org[i];
+        const double R = Rj[i] - 1.0 * 0.0;
+        const double fi = qt - qj_old[i] + dt * R;
+        const double f = 1.0 * fi;
+        d += f * f;
+      }
+      return 0.5 * d;
+    };
+    const double sf_thr = 0.9 * scal_f_old;
     double alam = 1.0;
-    int trial;
-    for (trial = 0; trial < 4096; ++trial) {
+    int trial = 0;
+    bool capped = true;   // the loop ran out of its 4096 trials
+    while (trial < 4096) {
+      if (trial > 0 && alam != 1.0 && xfin) {
+        const double alam_b = 0.5 * alam;
+        const double ha = partial_half_sum(alam);
+        const double hb = partial_half_sum(alam_b);
+        if (ha > sf_thr) {            // trial `trial` fails
+          ++trials;
+          if (alam < alamin) {
+            capped = false;
+            stale = true;
+            break;
+          }
+          alam = alam_b;
+          if (++trial >= 4096) break;
+          if (alam != 1.0 && hb > sf_thr) {   // and so does the next one
+            ++trials;
+            if (alam < alamin) {
+              capped = false;
+              stale = true;
+              break;
+            }
+            alam = 0.5 * alam;
+            ++trial;
+            continue;
+          }
+        }
+      }
+      // a trial with the full residual
       double qt[NV];
 #pragma unroll
       for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i] + alam * dd[i];
 #pragma unroll
       for (int i = 0; i < NV; ++i) qt[i] = qj_rel[i] * qj_org[i];
-      // Rows other than 2, 3 carry no implicit term: eval_f's sum of f^2
-      // taken over them alone, in eval_f's order, cannot exceed the full
-      // sum (rounded addition of a term >= 0 never decreases a sum, and
-      // rounding is monotone).  When that partial half-sum already exceeds
-      // 0.9*scal_f_old the trial fails whatever the implicit terms are, and
-      // the implicit terms are not evaluated.  Only for trials whose failure
-      // is all that matters: not trial 0 and not alam = 1 (their scal_f
-      // sets the next alam), and with a finite old iterate (then the
-      // residual left by the last trial is never read: a search that puts
-      // the old iterate back ends the iteration as converged).
-      bool fails = false;
-      if (trial > 0 && alam != 1.0 && xfin) {
-        double d = 0.0;
-#pragma unroll
-        for (int i = 0; i < NV; ++i) {
-          if (i == 1 || i == 2) continue;
-          const double R = Rj[i] - 1.0 * 0.0;
-          const double fi = qt[i] - qj_old[i] + dt * R;
-          const double f = 1.0 * fi;
-          d += f * f;
-        }
-        fails = 0.5 * d > 0.9 * scal_f_old;
-      }
-      if (!fails) eval_f<NS>(P, qt, qj_old, Rj, bx, by, dt, rt, scal_f);
+      eval_f<NS>(P, qt, qj_old, Rj, bx, by, dt, rt, scal_f);
       ++trials;
-      if (!fails && scal_f <= 0.9 * scal_f_old) break;
+      if (scal_f <= sf_thr) {
+        capped = false;
+        break;
+      }
       if (alam < alamin) {
-#pragma unroll
-        for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i];
-        scal_f = scal_f_old;
+        capped = false;
         stale = true;
         break;
       }
@@ -1087,8 +1140,10 @@ IMEX_FLAT bool newton_iterk(const DevParams& P, double* qj, const double* qj_old
       } else {
         alam = 0.5 * alam;
       }
+      ++trial;
     }
-    if (trial == 4096) {
+    if (stale || capped) {
+      // alam < alamin or the trial cap: the old iterate is put back
 #pragma unroll
       for (int i = 0; i < NV; ++i) qj_rel[i] = x_old[i];
       scal_f = scal_f_old;
@@ -1488,7 +1543,11 @@ __device__ __forceinline__ void stage2_first_lane(
           double Rj[NV];
 #pragma unroll
           for (int i = 0; i < NV; ++i) {
-            SI[i] = (qsi[i] - qfv[i]) / (dt * 1.0);
+            // rows other than 2, 3: qsi = qfv + dt*0 (or +0 for qfv = -0), so
+            // for finite qfv and a finite dt > 0 the difference is +0 and so
+            // is the quotient
+            if (i != 1 && i != 2 && isfinite(qfv[i]) && dt > 0.0 && dt < 1e300) SI[i] = 0.0;
+            else SI[i] = (qsi[i] - qfv[i]) / (dt * 1.0);
             double sa = 0.0 + Xc[i] * 1.0;
             double sb = 0.0 + (0.0 + 0.0) * 0.0;
             Rj[i] = (sa - sb) - 1.0 * SI[i];

@@ -560,8 +560,9 @@ def point_eval(fn, a, b, c=None, d=None, g=0.0, fast=False):
     fn "ipow" gives a**b, fn "settling" settling_velocity(a, b, c, d) with
     gravity g, "minmod_uniform" the minmod slope of a, b, c at centres 0, d,
     2d by the flux kernel's equal-spacing path, "limit" limit() at those
-    centres with limiter g.  Arrays are broadcast to one shape."""
-    code = {"ipow": 0, "settling": 1, "minmod_uniform": 2, "limit": 3}[fn]
+    centres with limiter g, "quotient_below" 1.0 where a/b < c as the
+    kernels evaluate it, else 0.0.  Arrays are broadcast to one shape."""
+    code = {"ipow": 0, "settling": 1, "minmod_uniform": 2, "limit": 3, "quotient_below": 4}[fn]
     arrs = [np.ascontiguousarray(x, dtype=np.float64)
             for x in np.broadcast_arrays(a, b, *(() if code == 0 else (c, d)))]
     while len(arrs) < 4:

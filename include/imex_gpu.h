@@ -472,6 +472,8 @@ const char* imex_setup_last_error(void);
  *         by the equal-spacing path of the flux kernel
  *   fn 3  limit(a, b, c at centres 0, d, 2d) with limiter g (0..7), theta 1
  *         src/geometry_2d.f90:1555-1676
+ *   fn 4  the kernels' test of a rounded quotient against a threshold,
+ *         taken without the division where certain: 1 if a/b < c, else 0
  * Returns IMEX_EINVAL for another fn or n < 0, IMEX_ENODEVICE without a GPU. */
 int imex_gpu_point_eval(int fn, long long n, const double* a, const double* b, const double* c,
                         const double* d, double g, double* out);

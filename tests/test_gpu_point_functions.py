@@ -124,3 +124,31 @@ def test_limit_equals_oracle(limiter):
     same = _same_bits(g, o) | (np.isnan(g) & np.isnan(o))
     bad = np.flatnonzero(~same)
     assert bad.size == 0, [(v[:, i], dz[i], g[i], o[i]) for i in bad[:5]]
+
+
+def test_quotient_below_threshold_equals_ieee():
+    """The kernels' test of a rounded quotient against a threshold (the
+    settling loop's 1e-6, the Newton step's EPSILON), taken without the
+    division where the answer is certain, against numpy's IEEE division:
+    quotients next to the thresholds, both signs, zeros, infinities, NaN,
+    extreme magnitudes."""
+    rng = np.random.default_rng(21)
+    n = 1 << 21
+    b = np.exp(rng.uniform(np.log(1e-300), np.log(1e300), n)) * rng.choice([-1.0, 1.0], n)
+    b[: n // 4] = rng.uniform(-2.0, 2.0, n // 4)
+    c = np.where(rng.random(n) < 0.5, 1e-6, 2.220446049250313e-16)
+    # a = |b|*c*(1 + k*2^-52): quotients next to the threshold on either side
+    k = rng.integers(-6, 7, n).astype(np.float64)
+    a = np.abs(b) * c * (1.0 + k * 2.0 ** -52)
+    m = n // 2
+    a[m:] = np.exp(rng.uniform(np.log(1e-300), np.log(1e300), n - m)) * rng.choice([-1.0, 1.0], n - m)
+    specials = np.array([0.0, -0.0, 1.0, -1.0, np.inf, -np.inf, np.nan, 1e-310, 1e308])
+    sa, sb = np.meshgrid(specials, specials)
+    a = np.concatenate([a, sa.ravel()])
+    b = np.concatenate([b, sb.ravel()])
+    c = np.concatenate([c, np.full(sa.size, 1e-6)])
+    g = point_eval("quotient_below", a, b, c, c)
+    with np.errstate(all="ignore"):
+        want = (a / b < c).astype(np.float64)
+    bad = np.flatnonzero(g != want)
+    assert bad.size == 0, [(a[i], b[i], c[i], g[i], want[i]) for i in bad[:5]]
