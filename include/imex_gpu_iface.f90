@@ -361,6 +361,26 @@ MODULE imex_gpu_iface
        INTEGER(C_INT), INTENT(OUT) :: first_bad_member
      END FUNCTION imex_gpu_ensemble_advance
 
+     ! 0: batched when the members allow it, 2: per-member graphs on streams
+     INTEGER(C_INT) FUNCTION imex_gpu_ensemble_set_mode(ens, mode)          &
+          BIND(C, name="imex_gpu_ensemble_set_mode")
+       IMPORT :: C_INT, C_PTR
+       TYPE(C_PTR), VALUE :: ens
+       INTEGER(C_INT), VALUE :: mode
+     END FUNCTION imex_gpu_ensemble_set_mode
+
+     ! the batched mode's tile shape and the timed trial steps (up to cap)
+     INTEGER(C_INT) FUNCTION imex_gpu_ensemble_tile_shape(ens, tx, ty,       &
+          n_tried, tried_tx, tried_ty, tried_ms, cap)                        &
+          BIND(C, name="imex_gpu_ensemble_tile_shape")
+       IMPORT :: C_INT, C_FLOAT, C_PTR
+       TYPE(C_PTR), VALUE :: ens
+       INTEGER(C_INT), INTENT(OUT) :: tx, ty, n_tried
+       INTEGER(C_INT), INTENT(OUT) :: tried_tx(*), tried_ty(*)
+       REAL(C_FLOAT), INTENT(OUT) :: tried_ms(*)
+       INTEGER(C_INT), VALUE :: cap
+     END FUNCTION imex_gpu_ensemble_tile_shape
+
   END INTERFACE
 
 END MODULE imex_gpu_iface
