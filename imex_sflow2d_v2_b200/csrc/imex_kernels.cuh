@@ -55,10 +55,10 @@ constexpr int NYI = Shape32x8::NYI;
 
 // Minimum resident blocks per SM asked of ptxas for the flux and per-cell
 // kernels (their register budget); tuning knobs, set with -D at build time.
-// The Newton list passes run at 96 registers (5 blocks of 128): 9.8 ms per
-// step at 4096^2 against 9.9 at 80 registers and 10.3 at 64 and 72.
+// The Newton list passes run at 128 registers (4 blocks of 128): 7.34 ms
+// per step at 4096^2 against 7.63 at 96 registers and 7.79 at 80.
 #ifndef IMEX_STAGE2_MINB
-#define IMEX_STAGE2_MINB 5
+#define IMEX_STAGE2_MINB 4
 #endif
 #ifndef IMEX_EROSION_MINB
 #define IMEX_EROSION_MINB 8
