@@ -747,17 +747,43 @@ def main():
         g.sync()
         if dist:
             dist.barrier()
+        # one untimed call: the first one on a context creates its transfer
+        # stream and events and loads the band kernels
+        g.advance_host(hq, 0.0, out=hq)
+        hq[:] = np.asarray(q0).ravel(order="F")
+        g.set_clock(0.0, 1e-2)
+        g.sync()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            g.advance_host(hq, 0.0, out=hq)
+        g.sync()
+        el = time.perf_counter() - t0
+        e2e_rate, el = job_rate(el, cells * args.e2e_steps, dist, "cuda")
+        # the same steps as three calls (state up, step, state down), whose
+        # transfers cannot overlap the step
+        hq[:] = np.asarray(q0).ravel(order="F")
+        g.set_clock(0.0, 1e-2)
+        g.sync()
+        if dist:
+            dist.barrier()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
             g.set_state(hq, 0.0)
             g.advance(1)
             g.get_state(out=hq)
         g.sync()
-        el = time.perf_counter() - t0
-        e2e_rate, el = job_rate(el, cells * args.e2e_steps, dist, "cuda")
+        el3 = time.perf_counter() - t0
+        calls_rate, _ = job_rate(el3, cells * args.e2e_steps, dist, "cuda")
         e2e = {"value": e2e_rate, "unit": UNIT,
                "h2d_bytes_per_step": nv * cells * 8, "d2h_bytes_per_step": nv * cells * 8,
-               "steps": args.e2e_steps}
+               "steps": args.e2e_steps,
+               "api": "imex_gpu_advance_host (pinned host q in and out, transfers in row "
+                      "bands overlapped with the step)",
+               "three_calls": {"value": calls_rate, "unit": UNIT,
+                               "api": "imex_gpu_set_state + imex_gpu_advance(1) + "
+                                      "imex_gpu_get_state"}}
 
     fast = None
     if rank == 0 and world == 1 and not args.no_fast:

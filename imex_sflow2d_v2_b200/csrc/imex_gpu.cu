@@ -33,6 +33,10 @@ struct ImexCtx {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;  // created by the context
+  // host-state steps (imex_gpu_advance_host): the transfer stream and its
+  // band events, created on first use
+  cudaStream_t copy_stream = nullptr;
+  std::vector<cudaEvent_t> band_ev;
   DevParams P{};
   DevParams* dP = nullptr;      // device copy of P
   ImexParams host_params{};
@@ -381,6 +385,143 @@ cudaError_t enqueue_step(ImexCtx* ctx) {
   k_step_end<<<1, 1, 0, ctx->stream>>>(ctx->clk);
   ctx->launches += 1;
   return cudaGetLastError();
+}
+
+// Row bands of imex_gpu_advance_host: more bands shorten the pipeline's fill
+// and drain (the first band's upload and the last band's download, which
+// nothing overlaps) at a few more launches per band.  At 4096^2 a step from
+// and to pinned host memory took 54.0, 49.6 and 47.4 ms with 4, 8 and 16
+// bands (63.7 ms as three calls).
+#ifndef IMEX_HOST_BANDS
+#define IMEX_HOST_BANDS 16
+#endif
+constexpr int kHostBands = IMEX_HOST_BANDS;
+
+// One driver-loop pass from a host state to a host state, the transfers
+// overlapped with the step in row bands.  The bands' host->device copies
+// run on the transfer stream; as band b has arrived and been converted,
+// the mask of band b-1 and the fluxes of band b-2 run (the mask needs two
+// rows of q beyond its band, the fluxes two rows of mask and q).  Stage 2
+// up to the Newton passes needs the global dt and runs on the whole grid;
+// then each band's assembly and erosion/deposition run and its rows go
+// back to the host while the next band computes.  Every cell sees the
+// kernels and operations of enqueue_step, in the same order per cell.
+template <int NS>
+cudaError_t enqueue_host_step_ns(ImexCtx* ctx, const double* q_in, double* q_out) {
+  const DevParams& P = ctx->P;
+  cudaStream_t st = ctx->stream, cs = ctx->copy_stream;
+  const int tiles_x = (P.nx + TX - 1) / TX, tiles_y = (P.ny + TY - 1) / TY;
+  const int nb = std::min(kHostBands, tiles_y);
+  std::vector<int> tb(nb + 1);
+  for (int b = 0; b <= nb; ++b) tb[b] = (int)((long long)b * tiles_y / nb);
+  auto r0 = [&](int b) { return tb[b] * TY; };
+  auto r1 = [&](int b) { return std::min(tb[b + 1] * TY, P.ny); };
+  const size_t row = (size_t)P.nx * P.nv;   // doubles of one AoS grid row
+  cudaEvent_t* ev = ctx->band_ev.data();    // [0] start, [1..nb] in, [nb+1..2nb] out
+  cudaError_t e;
+  // nothing earlier on the stream may still read the staging buffer
+  if ((e = cudaEventRecord(ev[0], st)) != cudaSuccess) return e;
+  if ((e = cudaStreamWaitEvent(cs, ev[0], 0)) != cudaSuccess) return e;
+  for (int b = 0; b < nb; ++b) {
+    const size_t off = (size_t)r0(b) * row, bytes = (size_t)(r1(b) - r0(b)) * row * sizeof(double);
+    if ((e = cudaMemcpyAsync(ctx->scratch + off, q_in + off, bytes, cudaMemcpyHostToDevice, cs)) !=
+        cudaSuccess)
+      return e;
+    if ((e = cudaEventRecord(ev[1 + b], cs)) != cudaSuccess) return e;
+  }
+  k_step_begin<<<1, 1, 0, st>>>(ctx->clk, P.max_dt, 1);
+  const size_t smem = sizeof(FluxShared<NS>);
+  static std::atomic<unsigned long long> attr_set{0};
+  if (attr_needed(attr_set)) {
+    if ((e = cudaFuncSetAttribute(k_flux_rows<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem)) != cudaSuccess)
+      return e;
+    if ((e = cudaFuncSetAttribute(k_flux_rows<NS>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  (int)cudaSharedmemCarveoutMaxShared)) != cudaSuccess)
+      return e;
+    attr_done(attr_set);
+  }
+  int launches = 1;
+  auto mask_band = [&](int b) {
+    k_mask_rows<<<dim3(tiles_x, tb[b + 1] - tb[b]), 256, 0, st>>>(
+        ctx->P, ctx->q, ctx->release, ctx->cellinfo, ctx->clk, ctx->mask, ctx->clk, tb[b]);
+    ++launches;
+  };
+  auto flux_band = [&](int b) {
+    k_flux_rows<NS><<<dim3(tiles_x, tb[b + 1] - tb[b]), FLUX_THREADS, smem, st>>>(
+        ctx->P, ctx->q, ctx->mask, ctx->cellinfo, ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy, ctx->Byy,
+        ctx->gc, ctx->dgc, ctx->gcsx, ctx->gcsy, ctx->ring, ctx->clk, ctx->X, tb[b]);
+    ++launches;
+  };
+  for (int b = 0; b < nb; ++b) {
+    if ((e = cudaStreamWaitEvent(st, ev[1 + b], 0)) != cudaSuccess) return e;
+    const int rows = r1(b) - r0(b);
+    k_aos_to_soa<<<grid_1d((long long)rows * row, 256), 256, 0, st>>>(
+        ctx->scratch + (size_t)r0(b) * row, ctx->q + (size_t)r0(b) * P.pitch, P.nv, P.nx, rows,
+        P.pitch, P.plane);
+    ++launches;
+    if (b >= 1) mask_band(b - 1);
+    if (b >= 2) flux_band(b - 2);
+  }
+  mask_band(nb - 1);
+  if (nb >= 2) flux_band(nb - 2);
+  flux_band(nb - 1);
+  k_dt_clip<<<1, 1, 0, st>>>(ctx->clk, 1);
+  ++launches;
+  // stage 2 through the Newton passes (launch_stage2_ns without assembly)
+  const long long ncell = (long long)P.nx * P.ny;
+  const int grid = grid_1d(ncell, STAGE2_THREADS);
+  const int lgrid = std::min(grid, 148 * IMEX_STAGE2_MINB);
+  k_nw_reset<<<1, 1, 0, st>>>(ctx->clk);
+  k_stage2_first<NS><<<grid, STAGE2_THREADS, 0, st>>>(ctx->P, ctx->q, ctx->X, ctx->mask, ctx->Bx,
+                                                     ctx->By, ctx->Bxx, ctx->Bxy, ctx->Byy,
+                                                     ctx->gc, ctx->nw, ctx->clk);
+  k_stage2_iter<NS><<<lgrid, STAGE2_THREADS, 0, st>>>(ctx->P, ctx->q, ctx->Bx, ctx->By, ctx->nw,
+                                                     ctx->clk, 2);
+  k_stage2_iter<NS><<<lgrid, STAGE2_THREADS, 0, st>>>(ctx->P, ctx->q, ctx->Bx, ctx->By, ctx->nw,
+                                                     ctx->clk, 3);
+  k_stage2_tail<NS><<<lgrid, STAGE2_THREADS, 0, st>>>(ctx->P, ctx->q, ctx->Bx, ctx->By, ctx->nw,
+                                                     ctx->clk);
+  launches += 5;
+  const bool ero = erosion_active(ctx);
+  for (int b = 0; b < nb; ++b) {
+    const int k0 = r0(b), k1 = r1(b), rows = k1 - k0;
+    k_stage2_post_rows<NS><<<grid_1d((long long)rows * P.nx, STAGE2_THREADS), STAGE2_THREADS, 0,
+                             st>>>(ctx->P, ctx->q, ctx->mask, ctx->cellinfo, ctx->nw, ctx->clk, k0,
+                                   k1);
+    ++launches;
+    if (ero) {
+      k_erosion_rows<NS><<<grid_1d((long long)rows * P.nx, 128), 128, 0, st>>>(
+          ctx->P, ctx->q, ctx->mask, ctx->Bx, ctx->By, ctx->erodible, ctx->deposit, ctx->erosion,
+          ctx->Bcent, ctx->clk, k0, k1);
+      ++launches;
+    }
+    if (b == nb - 1) {
+      k_step_end<<<1, 1, 0, st>>>(ctx->clk);
+      ++launches;
+    }
+    k_soa_to_aos<<<grid_1d((long long)rows * row, 256), 256, 0, st>>>(
+        ctx->q + (size_t)k0 * P.pitch, ctx->scratch + (size_t)k0 * row, P.nv, P.nx, rows, P.pitch,
+        P.plane);
+    ++launches;
+    if ((e = cudaEventRecord(ev[1 + nb + b], st)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(cs, ev[1 + nb + b], 0)) != cudaSuccess) return e;
+    const size_t off = (size_t)k0 * row;
+    if ((e = cudaMemcpyAsync(q_out + off, ctx->scratch + off, (size_t)rows * row * sizeof(double),
+                             cudaMemcpyDeviceToHost, cs)) != cudaSuccess)
+      return e;
+  }
+  ctx->launches += launches;
+  return cudaGetLastError();
+}
+
+cudaError_t enqueue_host_step(ImexCtx* ctx, const double* q_in, double* q_out) {
+  switch (ctx->ns) {
+    case 1: return enqueue_host_step_ns<1>(ctx, q_in, q_out);
+    case 2: return enqueue_host_step_ns<2>(ctx, q_in, q_out);
+    case 3: return enqueue_host_step_ns<3>(ctx, q_in, q_out);
+    default: return enqueue_host_step_ns<4>(ctx, q_in, q_out);
+  }
 }
 
 int validate(const ImexParams* p, std::string& why) {
@@ -748,6 +889,11 @@ int imex_gpu_destroy(ImexCtx* ctx) {
     if (b) cudaFree(b);
   if (ctx->clk_host) cudaFreeHost(ctx->clk_host);
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
+  for (cudaEvent_t e : ctx->band_ev) cudaEventDestroy(e);
+  if (ctx->copy_stream) {
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamDestroy(ctx->copy_stream);
+  }
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
   return IMEX_OK;
@@ -970,6 +1116,36 @@ int imex_gpu_advance(ImexCtx* ctx, int n_steps, int use_graph, double* t) {
   }
   int r = collect_errors(ctx);
   return r;
+}
+
+int imex_gpu_advance_host(ImexCtx* ctx, const double* q_in, double t, double* q_out,
+                          double* t_out) {
+  if (!ctx || !q_in || !q_out) return IMEX_EINVAL;
+  CK(cudaSetDevice(ctx->device));
+  if (ctx->nw.warm || ctx->nw.harvest || ctx->P.topo_change_flag || ctx->post_on || ctx->prof) {
+    // options the banded step leaves out: the three calls in sequence
+    int r = imex_gpu_set_state(ctx, q_in, t);
+    if (r) return r;
+    const int ra = imex_gpu_advance(ctx, 1, 0, t_out);
+    if (ra >= IMEX_ETIMEOUT) return ra;
+    r = imex_gpu_get_state(ctx, q_out, nullptr);
+    return r ? r : ra;
+  }
+  if (!ctx->copy_stream) CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+  while (ctx->band_ev.size() < (size_t)(2 * kHostBands + 1)) {
+    cudaEvent_t ev;
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    ctx->band_ev.push_back(ev);
+  }
+  int r = push_time(ctx, t, nullptr);
+  if (r) return r;
+  ctx->x_valid = false;
+  cudaError_t e = enqueue_host_step(ctx, q_in, q_out);
+  if (e != cudaSuccess) return fail(ctx, IMEX_ECUDA, cudaGetErrorString(e));
+  CK(cudaStreamSynchronize(ctx->copy_stream));
+  if (t_out)
+    CK(cudaMemcpyAsync(t_out, &ctx->clk->t, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  return collect_errors(ctx);
 }
 
 int imex_gpu_stats(ImexCtx* ctx, ImexStats* st, int reset_errors) {

@@ -178,6 +178,20 @@ __global__ void __launch_bounds__(256) k_mask(const __grid_constant__ DevParams 
                        blockIdx.x * TX, blockIdx.y * TY, s0, s1);
 }
 
+// k_mask over the tile rows [ty0, ty0 + gridDim.y): one band of a step whose
+// state arrives from the host band by band (imex_gpu_advance_host).
+__global__ void __launch_bounds__(256) k_mask_rows(const __grid_constant__ DevParams Pp,
+                                                   const double* __restrict__ q1,
+                                                   const double* __restrict__ release_time,
+                                                   const uint8_t* __restrict__ cellinfo,
+                                                   const DevClock* clk, uint8_t* __restrict__ mask,
+                                                   DevClock* clkw, int ty0) {
+  __shared__ uint8_t s0[SH][SW];
+  __shared__ uint8_t s1[SH][SW];
+  mask_tile<Shape32x8>(Pp, q1, release_time, cellinfo, clk->t, mask, clkw, 0, blockIdx.x * TX,
+                       (blockIdx.y + ty0) * TY, s0, s1);
+}
+
 // ================================================================== faces
 // Shared tile of physical states: qps[v][ly][lx]; info_s[ly][lx] holds the
 // cellinfo bits plus bit 7 = solve mask.
@@ -771,6 +785,23 @@ __global__ void __launch_bounds__(FLUX_THREADS, flux_min_blocks<NS>())
   FluxShared<NS>& S = *reinterpret_cast<FluxShared<NS>*>(smem_raw);
   flux_tile<NS, Shape32x8>(Pp, q, mask, cellinfo, Bx, By, Bxx, Bxy, Byy, gc, dgc, gcsx, gcsy, ring,
                            clk, X, blockIdx.x * TX, blockIdx.y * TY, S);
+}
+
+// k_flux over the tile rows [ty0, ty0 + gridDim.y) (imex_gpu_advance_host).
+template <int NS>
+__global__ void __launch_bounds__(FLUX_THREADS, flux_min_blocks<NS>())
+    k_flux_rows(const __grid_constant__ DevParams Pp, const double* __restrict__ q,
+                const uint8_t* __restrict__ mask, const uint8_t* __restrict__ cellinfo,
+                const double* __restrict__ Bx, const double* __restrict__ By,
+                const double* __restrict__ Bxx, const double* __restrict__ Bxy,
+                const double* __restrict__ Byy, const double* __restrict__ gc,
+                const double* __restrict__ dgc, const double* __restrict__ gcsx,
+                const double* __restrict__ gcsy, const RingCell* __restrict__ ring, DevClock* clk,
+                double* __restrict__ X, int ty0) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FluxShared<NS>& S = *reinterpret_cast<FluxShared<NS>*>(smem_raw);
+  flux_tile<NS, Shape32x8>(Pp, q, mask, cellinfo, Bx, By, Bxx, Bxy, Byy, gc, dgc, gcsx, gcsy, ring,
+                           clk, X, blockIdx.x * TX, (blockIdx.y + ty0) * TY, S);
 }
 
 // =============================================================== Newton
@@ -2081,6 +2112,23 @@ __global__ void __launch_bounds__(STAGE2_THREADS)
   }
 }
 
+// k_stage2_post over the grid rows [k0, k1) (imex_gpu_advance_host).
+template <int NS>
+__global__ void __launch_bounds__(STAGE2_THREADS)
+    k_stage2_post_rows(const __grid_constant__ DevParams Pp, double* __restrict__ q,
+                       const uint8_t* __restrict__ mask, const uint8_t* __restrict__ cellinfo,
+                       NewtonWork W, DevClock* clk, int k0, int k1) {
+  const DevParams& P = Pp;
+  const int nx = P.nx;
+  const long long ncell = (long long)nx * (k1 - k0);
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < ncell;
+       g += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(g % nx), k = k0 + (int)(g / nx);
+    if (!mask[(size_t)k * P.pitch + j]) continue;
+    stage2_post_cell<NS>(P, q, cellinfo, W, clk, j, k);
+  }
+}
+
 // Stand-alone erosion/deposition pass (imex_gpu_erosion_deposition).
 template <int NS>
 __device__ __forceinline__ void erosion_update_cell(const DevParams& P, double* __restrict__ q,
@@ -2134,6 +2182,26 @@ __global__ void __launch_bounds__(128, IMEX_EROSION_MINB)
   for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < ncell;
        g += (long long)gridDim.x * blockDim.x) {
     int j = (int)(g % nx), k = (int)(g / nx);
+    if (!mask[(size_t)k * P.pitch + j]) continue;
+    erosion_update_cell<NS>(P, q, Bx, By, erodible, deposit, erosion, Bcent, clk, dt, j, k);
+  }
+}
+
+// k_erosion over the grid rows [k0, k1) (imex_gpu_advance_host).
+template <int NS>
+__global__ void __launch_bounds__(128, IMEX_EROSION_MINB)
+    k_erosion_rows(const __grid_constant__ DevParams Pp, double* __restrict__ q,
+                   const uint8_t* __restrict__ mask, const double* __restrict__ Bx,
+                   const double* __restrict__ By, double* __restrict__ erodible,
+                   double* __restrict__ deposit, double* __restrict__ erosion,
+                   double* __restrict__ Bcent, DevClock* clk, int k0, int k1) {
+  const DevParams& P = Pp;
+  const int nx = P.nx;
+  const long long ncell = (long long)nx * (k1 - k0);
+  const double dt = clk->dt;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < ncell;
+       g += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(g % nx), k = k0 + (int)(g / nx);
     if (!mask[(size_t)k * P.pitch + j]) continue;
     erosion_update_cell<NS>(P, q, Bx, By, erodible, deposit, erosion, Bcent, clk, dt, j, k);
   }

@@ -62,6 +62,7 @@ def load_library(path=None, fast=False):
         "imex_gpu_get_masks": ([vp, i8p, i8p, i8p], C.c_int),
         "imex_gpu_set_clock": ([vp, C.c_double, C.c_double, C.c_double, C.c_double], C.c_int),
         "imex_gpu_advance": ([vp, C.c_int, C.c_int, dp], C.c_int),
+        "imex_gpu_advance_host": ([vp, dp, C.c_double, dp, dp], C.c_int),
         "imex_gpu_stats": ([vp, C.POINTER(ImexStats), C.c_int], C.c_int),
         "imex_gpu_last_error": ([vp], C.c_char_p),
         "imex_gpu_sync": ([vp], C.c_int),
@@ -341,6 +342,26 @@ class ImexSolver:
         rc = self._check(self.lib.imex_gpu_advance(self._h, int(n_steps), int(bool(use_graph)),
                                                    C.byref(t)), "advance")
         return rc, t.value
+
+    def advance_host(self, q, t, out=None):
+        """One driver-loop pass from the host state q at time t to the host
+        state after it (imex_gpu_advance_host: the same result as set_state,
+        advance(1) and get_state, with the transfers overlapped by the step).
+        q and `out` as for set_state/get_state (flat float64 arrays in
+        Fortran element order are used as they are; they may be the same
+        array).  Returns (status, q after the step, t after the step)."""
+        if not (isinstance(q, np.ndarray) and q.ndim == 1 and q.dtype == np.float64
+                and q.flags.c_contiguous):
+            q = np.ascontiguousarray(np.asarray(q, dtype=np.float64).ravel(order="F"))
+        shaped = out is None
+        if out is None:
+            out = np.empty(self.nv * self.nx * self.ny)
+        tt = C.c_double(0.0)
+        rc = self._check(self.lib.imex_gpu_advance_host(self._h, _p(q), float(t), _p(out),
+                                                        C.byref(tt)), "advance_host")
+        if shaped:
+            out = out.reshape((self.nv, self.nx, self.ny), order="F")
+        return rc, out, tt.value
 
     def stats(self, reset_errors=False):
         s = ImexStats()

@@ -13,6 +13,7 @@
  *                                                                src/solver_2d.f90:2380-2595
  *   imex_gpu_set_state/get_state  <- the module arrays q, qp     src/solver_2d.f90:68,157
  *   imex_gpu_advance              <- one pass of the driver loop src/IMEX_SfloW2D.f90:337-389
+ *   imex_gpu_advance_host         <- the same pass with q held on the host
  *                                    (check_solve, timestep, dt clipping, imex_RK_solver,
  *                                     update_erosion_deposition_cell, t = t + dt)
  *
@@ -228,6 +229,25 @@ int imex_gpu_get_masks(ImexCtx* ctx, int8_t* solve_mask, int8_t* mask_x, int8_t*
  */
 int imex_gpu_set_clock(ImexCtx* ctx, double t, double dt0, double t_end, double t_output);
 int imex_gpu_advance(ImexCtx* ctx, int n_steps, int use_graph, double* t);
+
+/*
+ * One pass of the driver loop (src/IMEX_SfloW2D.f90:339-389) for a driver
+ * that keeps q on the host, as the reference's module arrays are: the result
+ * of imex_gpu_set_state(ctx, q_in, t); imex_gpu_advance(ctx, 1, 0, t_out);
+ * imex_gpu_get_state(ctx, q_out, NULL), bit for bit, with the transfers
+ * overlapped with the step.  The grid goes up and comes back in row bands
+ * on a second stream: the masks and fluxes of a band start as soon as the
+ * band and its neighbour rows are on the device, and a band's rows return
+ * once its assembly and erosion/deposition are done (stage 2's Newton
+ * passes, which wait for the global dt, run on the whole grid in between).
+ * q_in and q_out are q(n_vars, nx, ny) in Fortran order and may be the same
+ * array; page-locked host memory lets the copies overlap.  Returns like
+ * imex_gpu_advance (a reference check's code after the step completed).
+ * With a warm start, harvest, moving bed, output sweep or profiling on, the
+ * three calls run one after the other.  Synchronous.
+ */
+int imex_gpu_advance_host(ImexCtx* ctx, const double* q_in, double t, double* q_out,
+                          double* t_out);
 
 int imex_gpu_stats(ImexCtx* ctx, ImexStats* st, int reset_errors);
 const char* imex_gpu_last_error(ImexCtx* ctx);

@@ -221,6 +221,18 @@ MODULE imex_gpu_iface
        REAL(C_DOUBLE), INTENT(OUT) :: t
      END FUNCTION imex_gpu_advance
 
+     ! one driver-loop pass with q kept on the host: q_in at time t in, the
+     ! state after the step out (may be the same array), transfers overlapped
+     INTEGER(C_INT) FUNCTION imex_gpu_advance_host(ctx, q_in, t, q_out,      &
+          t_out) BIND(C, name="imex_gpu_advance_host")
+       IMPORT :: C_INT, C_PTR, C_DOUBLE
+       TYPE(C_PTR), VALUE :: ctx
+       REAL(C_DOUBLE), INTENT(IN) :: q_in(*)
+       REAL(C_DOUBLE), VALUE :: t
+       REAL(C_DOUBLE), INTENT(INOUT) :: q_out(*)
+       REAL(C_DOUBLE), INTENT(OUT) :: t_out
+     END FUNCTION imex_gpu_advance_host
+
      INTEGER(C_INT) FUNCTION imex_gpu_stats(ctx, st, reset_errors)             &
           BIND(C, name="imex_gpu_stats")
        IMPORT :: C_INT, C_PTR, imex_stats
