@@ -126,7 +126,7 @@ template <int NS, class TS>
 __global__ void __launch_bounds__(TS::THREADS, (flux_min_blocks<NS, TS>()))
     kb_flux(const MemberDev* __restrict__ M, const uint32_t* __restrict__ tile_member,
             const uint32_t* __restrict__ active, const unsigned int* __restrict__ n_active) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   FluxShared<NS, TS>& S = *reinterpret_cast<FluxShared<NS, TS>*>(smem_raw);
   DevParams& sP = *reinterpret_cast<DevParams*>(smem_raw + sizeof(FluxShared<NS, TS>));
   const unsigned int n = *n_active;

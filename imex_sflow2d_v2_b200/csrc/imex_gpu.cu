@@ -37,6 +37,9 @@ struct ImexCtx {
   // band events, created on first use
   cudaStream_t copy_stream = nullptr;
   std::vector<cudaEvent_t> band_ev;
+  // tensor map of q for the flux kernel's TMA tile loads (k_flux_tma)
+  alignas(64) CUtensorMap q_tmap{};
+  bool q_tmap_ok = false;
   DevParams P{};
   DevParams* dP = nullptr;      // device copy of P
   ImexParams host_params{};
@@ -192,10 +195,59 @@ struct ProfScope {
 };
 
 // ------------------------------------------------------- launch helpers
+// The tensor map of q for k_flux_tma: dims {nx, ny, n_v} in elements, row
+// and plane strides in bytes (multiples of 16: the pitch is a multiple of
+// 16 elements), box {SW, SH, n_v} = the flux tile with its halo, zero fill
+// outside the grid.  The encoder comes from the driver through the
+// runtime; without it (or if it refuses the map) k_flux loads the tile
+// itself.
+bool encode_q_map(ImexCtx* ctx) {
+  typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                    const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                    const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                    CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult qr;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &qr) !=
+          cudaSuccess ||
+      qr != cudaDriverEntryPointSuccess || !fn)
+    return false;
+  const DevParams& P = ctx->P;
+  if ((P.pitch * sizeof(double)) % 16 != 0 || (reinterpret_cast<uintptr_t>(ctx->q) % 16) != 0)
+    return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)P.nx, (cuuint64_t)P.ny, (cuuint64_t)P.nv};
+  const cuuint64_t strides[2] = {(cuuint64_t)P.pitch * sizeof(double),
+                                 (cuuint64_t)P.plane * sizeof(double)};
+  const cuuint32_t box[3] = {(cuuint32_t)SW, (cuuint32_t)SH, (cuuint32_t)P.nv};
+  const cuuint32_t elem[3] = {1, 1, 1};
+  const CUresult r = reinterpret_cast<EncodeTiledFn>(fn)(
+      &ctx->q_tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, ctx->q, dims, strides, box, elem,
+      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
 template <int NS>
 cudaError_t launch_flux_ns(ImexCtx* ctx) {
   const DevParams& P = ctx->P;
   size_t smem = sizeof(FluxShared<NS>);
+  if (ctx->q_tmap_ok) {
+    static std::atomic<unsigned long long> attr_tma{0};
+    if (attr_needed(attr_tma)) {
+      cudaError_t e = cudaFuncSetAttribute(k_flux_tma<NS>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      e = cudaFuncSetAttribute(k_flux_tma<NS>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               (int)cudaSharedmemCarveoutMaxShared);
+      if (e != cudaSuccess) return e;
+      attr_done(attr_tma);
+    }
+    k_flux_tma<NS><<<tile_grid(P), FLUX_THREADS, smem, ctx->stream>>>(
+        ctx->P, ctx->q_tmap, ctx->q, ctx->mask, ctx->cellinfo, ctx->Bx, ctx->By, ctx->Bxx,
+        ctx->Bxy, ctx->Byy, ctx->gc, ctx->dgc, ctx->gcsx, ctx->gcsy, ctx->ring, ctx->clk, ctx->X);
+    ctx->launches += 1;
+    return cudaGetLastError();
+  }
   static std::atomic<unsigned long long> attr_set{0};
   if (attr_needed(attr_set)) {
     cudaError_t e = cudaFuncSetAttribute(k_flux<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -779,6 +831,7 @@ int imex_gpu_create(const ImexParams* p, const ImexStatic* s, int device, ImexCt
     return IMEX_EUNSUPPORTED;  // stage-2 cell lists hold 32-bit plane indices
   }
   CK(dalloc(&ctx->q, plane * nv));
+  ctx->q_tmap_ok = encode_q_map(ctx);
   CK(dalloc(&ctx->X, plane * nv));
   CK(dalloc(&ctx->mask, plane));
   CK(cudaMemset(ctx->q, 0, plane * nv * sizeof(double)));
@@ -1017,7 +1070,7 @@ static int collect_errors(ImexCtx* ctx) {
   uint32_t fresh = em & ~ctx->error_mask_acc;
   ctx->error_mask_acc |= em;
   if (!fresh) return IMEX_OK;
-  for (int code = 1; code <= 6; ++code)
+  for (int code = 1; code <= 7; ++code)
     if (fresh & (1u << code)) return code;
   return IMEX_OK;
 }
@@ -2236,7 +2289,7 @@ __global__ void __launch_bounds__(FLUX_THREADS)
                 const RingCell* __restrict__ ring, const DevClock* clk, double* tile_min) {
   constexpr int NV = 4 + NS, NP = 6 + NS;
   const DevParams& P = Pp;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   CflShared<NS>& S = *reinterpret_cast<CflShared<NS>*>(smem_raw);
   const int j0 = blockIdx.x * TX, k0 = blockIdx.y * TY;
   const int nx = P.nx, ny = P.ny;

@@ -20,6 +20,8 @@
 
 #include <type_traits>
 
+#include <cuda.h>   // CUtensorMap (the type only; maps are encoded by the host)
+
 #include "imex_device.cuh"
 #include "imex_mlp.cuh"
 
@@ -176,6 +178,52 @@ __global__ void __launch_bounds__(256) k_mask(const __grid_constant__ DevParams 
   __shared__ uint8_t s1[SH][SW];
   mask_tile<Shape32x8>(Pp, q1, release_time, cellinfo, clk->t, mask, clkw, solve_all,
                        blockIdx.x * TX, blockIdx.y * TY, s0, s1);
+}
+
+// ------------------------------------------------------ TMA tile loads
+// One bulk tensor copy per tile (cp.async.bulk.tensor, this GPU's memory
+// only, no multicast) completing on a shared-memory mbarrier.  The wait is
+// bounded: past the limit the caller records IMEX_ETIMEOUT (never expected).
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+// makes the barrier's initialisation visible to the copy engine's proxy
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y,
+                                            int z, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+constexpr int TMA_WAIT_LIMIT = 1 << 22;   // try_wait polls (seconds at most)
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, uint32_t phase) {
+  for (int it = 0; it < TMA_WAIT_LIMIT; ++it)
+    if (mbar_try_wait(bar, phase)) return true;
+  return false;
 }
 
 // k_mask over the tile rows [ty0, ty0 + gridDim.y): one band of a step whose
@@ -528,7 +576,12 @@ IMEX_FLAT void interface_flux(const DevParams& P, const Tile<NS, TS>& T, int dir
 template <int NS, class TS = Shape32x8>
 struct FluxShared {
   Tile<NS, TS> tile;
-  SlopeTile<NS, TS> slopes;
+  union {
+    SlopeTile<NS, TS> slopes;
+    // the tile's conserved variables as one TMA box (k_flux_tma), read
+    // before the slopes are first written
+    alignas(128) double stage[4 + NS][TS::SH][TS::SW];
+  };
   union {
     double Hx[4 + NS][TS::TY][TS::TX + 1];
     double Hy[4 + NS][TS::TY + 1][TS::TX];
@@ -538,6 +591,7 @@ struct FluxShared {
     double ay[TS::TY + 1][TS::TX];
   } A;
   double dtmin[TS::THREADS / 32];
+  unsigned long long tma_bar;   // mbarrier of the TMA box
 };
 static_assert(Shape32x8::THREADS == 288, "k_flux blocks of 288 threads for 32x8 tiles");
 
@@ -585,7 +639,8 @@ __device__ __forceinline__ void flux_tile(const DevParams& P, const double* __re
                                           const double* __restrict__ gcsy,
                                           const RingCell* __restrict__ ring, DevClock* clk,
                                           double* __restrict__ X, int j0, int k0,
-                                          FluxShared<NS, TS>& S) {
+                                          FluxShared<NS, TS>& S,
+                                          const CUtensorMap* qmap = nullptr) {
   constexpr int NV = 4 + NS, NP = 6 + NS;
   constexpr int TX = TS::TX, TY = TS::TY, SW = TS::SW, SH = TS::SH, NXI = TS::NXI,
                 NYI = TS::NYI;
@@ -598,6 +653,29 @@ __device__ __forceinline__ void flux_tile(const DevParams& P, const double* __re
     if (j < nx && k < ny && mask[(size_t)k * P.pitch + j]) any = 1;
   }
   if (!__syncthreads_or(any)) return;
+  // With a tensor map of q, the tile's n_v planes (halo included, zeros
+  // outside the grid) arrive as one TMA box in the staging area
+  const bool staged = qmap != nullptr;
+  if (staged) {
+    static_assert(sizeof(S.stage) == (size_t)(4 + NS) * SH * SW * sizeof(double), "box size");
+    if (threadIdx.x == 0) {
+      mbar_init(&S.tma_bar, 1);
+      fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      mbar_expect_tx(&S.tma_bar, (uint32_t)sizeof(S.stage));
+      // x = j0 - 2 is even: 16-byte aligned for 8-byte elements
+      tma_load_3d(&S.stage[0][0][0], qmap, j0 - HALO, k0 - HALO, 0, &S.tma_bar);
+    }
+    const bool arrived = mbar_wait_bounded(&S.tma_bar, 0);
+    if (__syncthreads_or(!arrived)) {
+      // never expected: record it, wait (bounded) for the copy, and leave
+      if (threadIdx.x == 0) record_error(clk, 7, (long long)k0 * nx + j0);
+      mbar_wait_bounded(&S.tma_bar, 0);
+      return;
+    }
+  }
   // physical states of the tile + halo
   for (int e = threadIdx.x; e < SW * SH; e += blockDim.x) {
     int lx = e % SW, ly = e / SW;
@@ -615,7 +693,7 @@ __device__ __forceinline__ void flux_tile(const DevParams& P, const double* __re
         qpv[3] = P.T_ambient;
       } else {
 #pragma unroll
-        for (int i = 0; i < NV; ++i) qc[i] = q[c + (size_t)i * P.plane];
+        for (int i = 0; i < NV; ++i) qc[i] = staged ? S.stage[i][ly][lx] : q[c + (size_t)i * P.plane];
         cell_qp<NS>(P, qc, qpv);
       }
     } else {
@@ -781,10 +859,28 @@ __global__ void __launch_bounds__(FLUX_THREADS, flux_min_blocks<NS>())
            const double* __restrict__ gc, const double* __restrict__ dgc,
            const double* __restrict__ gcsx, const double* __restrict__ gcsy,
            const RingCell* __restrict__ ring, DevClock* clk, double* __restrict__ X) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   FluxShared<NS>& S = *reinterpret_cast<FluxShared<NS>*>(smem_raw);
   flux_tile<NS, Shape32x8>(Pp, q, mask, cellinfo, Bx, By, Bxx, Bxy, Byy, gc, dgc, gcsx, gcsy, ring,
                            clk, X, blockIdx.x * TX, blockIdx.y * TY, S);
+}
+
+// k_flux with the tile's q planes loaded by one TMA box (qmap: a tensor map
+// of q, dims {nx, ny, n_v}, box {SW, SH, n_v}, zero fill outside the grid).
+template <int NS>
+__global__ void __launch_bounds__(FLUX_THREADS, flux_min_blocks<NS>())
+    k_flux_tma(const __grid_constant__ DevParams Pp, const __grid_constant__ CUtensorMap qmap,
+               const double* __restrict__ q, const uint8_t* __restrict__ mask,
+               const uint8_t* __restrict__ cellinfo, const double* __restrict__ Bx,
+               const double* __restrict__ By, const double* __restrict__ Bxx,
+               const double* __restrict__ Bxy, const double* __restrict__ Byy,
+               const double* __restrict__ gc, const double* __restrict__ dgc,
+               const double* __restrict__ gcsx, const double* __restrict__ gcsy,
+               const RingCell* __restrict__ ring, DevClock* clk, double* __restrict__ X) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  FluxShared<NS>& S = *reinterpret_cast<FluxShared<NS>*>(smem_raw);
+  flux_tile<NS, Shape32x8>(Pp, q, mask, cellinfo, Bx, By, Bxx, Bxy, Byy, gc, dgc, gcsx, gcsy, ring,
+                           clk, X, blockIdx.x * TX, blockIdx.y * TY, S, &qmap);
 }
 
 // k_flux over the tile rows [ty0, ty0 + gridDim.y) (imex_gpu_advance_host).
@@ -798,7 +894,7 @@ __global__ void __launch_bounds__(FLUX_THREADS, flux_min_blocks<NS>())
                 const double* __restrict__ dgc, const double* __restrict__ gcsx,
                 const double* __restrict__ gcsy, const RingCell* __restrict__ ring, DevClock* clk,
                 double* __restrict__ X, int ty0) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   FluxShared<NS>& S = *reinterpret_cast<FluxShared<NS>*>(smem_raw);
   flux_tile<NS, Shape32x8>(Pp, q, mask, cellinfo, Bx, By, Bxx, Bxy, Byy, gc, dgc, gcsx, gcsy, ring,
                            clk, X, blockIdx.x * TX, (blockIdx.y + ty0) * TY, S);
