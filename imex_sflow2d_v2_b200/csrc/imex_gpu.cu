@@ -485,12 +485,14 @@ cudaError_t enqueue_host_step_ns(ImexCtx* ctx, const double* q_in, double* q_out
   const size_t smem = sizeof(FluxShared<NS>);
   static std::atomic<unsigned long long> attr_set{0};
   if (attr_needed(attr_set)) {
-    if ((e = cudaFuncSetAttribute(k_flux_rows<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem)) != cudaSuccess)
-      return e;
-    if ((e = cudaFuncSetAttribute(k_flux_rows<NS>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                  (int)cudaSharedmemCarveoutMaxShared)) != cudaSuccess)
-      return e;
+    for (const void* fn : {(const void*)k_flux_rows<NS>, (const void*)k_flux_tma_rows<NS>}) {
+      if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+          cudaSuccess)
+        return e;
+      if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    (int)cudaSharedmemCarveoutMaxShared)) != cudaSuccess)
+        return e;
+    }
     attr_done(attr_set);
   }
   int launches = 1;
@@ -500,9 +502,16 @@ cudaError_t enqueue_host_step_ns(ImexCtx* ctx, const double* q_in, double* q_out
     ++launches;
   };
   auto flux_band = [&](int b) {
-    k_flux_rows<NS><<<dim3(tiles_x, tb[b + 1] - tb[b]), FLUX_THREADS, smem, st>>>(
-        ctx->P, ctx->q, ctx->mask, ctx->cellinfo, ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy, ctx->Byy,
-        ctx->gc, ctx->dgc, ctx->gcsx, ctx->gcsy, ctx->ring, ctx->clk, ctx->X, tb[b]);
+    const dim3 g(tiles_x, tb[b + 1] - tb[b]);
+    if (ctx->q_tmap_ok)
+      k_flux_tma_rows<NS><<<g, FLUX_THREADS, smem, st>>>(
+          ctx->P, ctx->q_tmap, ctx->q, ctx->mask, ctx->cellinfo, ctx->Bx, ctx->By, ctx->Bxx,
+          ctx->Bxy, ctx->Byy, ctx->gc, ctx->dgc, ctx->gcsx, ctx->gcsy, ctx->ring, ctx->clk,
+          ctx->X, tb[b]);
+    else
+      k_flux_rows<NS><<<g, FLUX_THREADS, smem, st>>>(
+          ctx->P, ctx->q, ctx->mask, ctx->cellinfo, ctx->Bx, ctx->By, ctx->Bxx, ctx->Bxy,
+          ctx->Byy, ctx->gc, ctx->dgc, ctx->gcsx, ctx->gcsy, ctx->ring, ctx->clk, ctx->X, tb[b]);
     ++launches;
   };
   for (int b = 0; b < nb; ++b) {

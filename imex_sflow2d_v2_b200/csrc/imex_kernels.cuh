@@ -883,6 +883,24 @@ __global__ void __launch_bounds__(FLUX_THREADS, flux_min_blocks<NS>())
                            clk, X, blockIdx.x * TX, blockIdx.y * TY, S, &qmap);
 }
 
+// k_flux_tma over the tile rows [ty0, ty0 + gridDim.y) (imex_gpu_advance_host).
+template <int NS>
+__global__ void __launch_bounds__(FLUX_THREADS, flux_min_blocks<NS>())
+    k_flux_tma_rows(const __grid_constant__ DevParams Pp, const __grid_constant__ CUtensorMap qmap,
+                    const double* __restrict__ q, const uint8_t* __restrict__ mask,
+                    const uint8_t* __restrict__ cellinfo, const double* __restrict__ Bx,
+                    const double* __restrict__ By, const double* __restrict__ Bxx,
+                    const double* __restrict__ Bxy, const double* __restrict__ Byy,
+                    const double* __restrict__ gc, const double* __restrict__ dgc,
+                    const double* __restrict__ gcsx, const double* __restrict__ gcsy,
+                    const RingCell* __restrict__ ring, DevClock* clk, double* __restrict__ X,
+                    int ty0) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  FluxShared<NS>& S = *reinterpret_cast<FluxShared<NS>*>(smem_raw);
+  flux_tile<NS, Shape32x8>(Pp, q, mask, cellinfo, Bx, By, Bxx, Bxy, Byy, gc, dgc, gcsx, gcsy, ring,
+                           clk, X, blockIdx.x * TX, (blockIdx.y + ty0) * TY, S, &qmap);
+}
+
 // k_flux over the tile rows [ty0, ty0 + gridDim.y) (imex_gpu_advance_host).
 template <int NS>
 __global__ void __launch_bounds__(FLUX_THREADS, flux_min_blocks<NS>())

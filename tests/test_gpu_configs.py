@@ -14,7 +14,8 @@ erosion/deposition exchange, to a relative 1e-12.
   radial current     1024x1024 cells of 2 m, two solid classes, Voellmy,
                      2000 steps through advance() replayed from a CUDA graph
   fractal inlet      512x512 instance of the 4096^2 workload's generator
-                     (three classes, settling + erosion, 2 m layer), 60 steps
+                     (three classes, settling + erosion, 2 m layer), 60 steps;
+                     and the 4096^2 workload itself (16.8 M cells), 3 steps
 """
 import math
 
@@ -119,3 +120,14 @@ def test_fractal_inlet_512_60_steps():
                                    errors_ok=True)
     b = o.mass_budget()
     assert b[2] != 0.0        # erosion/deposition moved mass
+
+
+def test_fractal_inlet_4096_3_steps():
+    """The headline workload at its full size: 4096^2 cells of 10 m, the
+    three steps after its initial state, against the oracle on all host
+    threads (the GPU path through its TMA flux tiles)."""
+    p, st, q = configs.fractal_inlet(n=4096, initial_layer=2.0)
+    assert (p.nx, p.ny, p.n_solid) == (4096, 4096, 3)
+    o, g, worst = _advance_compare(p, st, q, 3, 1, use_graph=False, exchange=True,
+                                   errors_ok=True)
+    assert g.stats().solve_cells > 16_000_000
