@@ -264,38 +264,75 @@ def cpu_parity(args, device):
             "stale_wet_reads": int(o.stale_wet_reads()), "tolerance_rel_l1": 1e-10}
 
 
-def config_rates(args, device):
+CHUNK = 50
+
+
+def _oracle_config_rate(p, st, q, steps, budget_s):
+    """The oracle's timing build (all host threads) on a workload from its
+    initial state, advanced in chunks of CHUNK steps until `steps` are done
+    or `budget_s` seconds have passed: (steps done, seconds, threads)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    timing = orc.timing_build_usable()
+    orc.build(target=orc.TIMING if timing else orc.CHECKER)
+    threads = orc.lib(orc.TIMING if timing else orc.CHECKER).oracle_max_threads()
+    o = orc.Oracle(p, st, threads=threads, timing=timing)
+    o.set_state(q, 0.0)
+    o.set_clock(0.0, 1e-2)
+    done, el = 0, 0.0
+    while done < steps and el < budget_s:
+        n_ = min(CHUNK, steps - done)
+        t0 = time.perf_counter()
+        o.advance(n_)
+        el += time.perf_counter() - t0
+        done += n_
+    return done, el, int(threads)
+
+
+def config_rates(args, device, cpu=True):
     """Cell-updates/s of the first two workloads at their stated sizes and
     step counts, each run from its initial state through advance() replayed
-    from a CUDA graph (device time by CUDA events on the library's stream)."""
+    from a CUDA graph (device time by CUDA events on the library's stream,
+    one event per chunk of CHUNK steps).  With `cpu`, the oracle's timing
+    build runs the same workload from the same initial state on all host
+    threads for the stated steps or a time budget, whichever ends first, and
+    the GPU's time over those same first steps sits beside it."""
     import torch
     from imex_sflow2d_v2_b200 import configs
     from imex_sflow2d_v2_b200.solver import ImexSolver
     out = {}
-    for name, (p, st, q), steps in (
-            ("dambreak_200", configs.dambreak(), 500),
-            ("radial_current_1024", configs.radial_current(), 2000)):
+    for name, (p, st, q), steps, budget in (
+            ("dambreak_200", configs.dambreak(), 500, 30.0),
+            ("radial_current_1024", configs.radial_current(), 2000, 25.0)):
         g = ImexSolver(p, st, device=device)
         stream = torch.cuda.current_stream()
         g.set_stream(stream.cuda_stream)
         g.set_state(q, 0.0)
         g.set_clock(0.0, 1e-2)
         g.sync()
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        cells = 0
-        ev0.record(stream)
-        for chunk in range(0, steps, 100):
-            g.advance(min(100, steps - chunk), use_graph=True)
-        ev1.record(stream)
+        evs = [torch.cuda.Event(enable_timing=True)]
+        evs[0].record(stream)
+        for chunk in range(0, steps, CHUNK):
+            g.advance(min(CHUNK, steps - chunk), use_graph=True)
+            evs.append(torch.cuda.Event(enable_timing=True))
+            evs[-1].record(stream)
         torch.cuda.synchronize()
-        ms = ev0.elapsed_time(ev1)
+        ms = evs[0].elapsed_time(evs[-1])
         s_ = g.stats()
         out[name] = {"grid": [p.nx, p.ny], "steps": steps,
                      "value": p.nx * p.ny * steps / (ms * 1e-3), "unit": UNIT,
                      "ms_per_step": ms / steps, "solve_cells_last_step": int(s_.solve_cells),
                      "t_end": s_.t, "errors": int(s_.error_mask)}
         g.close()
+        if cpu:
+            done, el, threads = _oracle_config_rate(p, st, q, steps, budget)
+            gms = evs[0].elapsed_time(evs[(done + CHUNK - 1) // CHUNK])
+            cv = p.nx * p.ny * done / el
+            gv = p.nx * p.ny * done / (gms * 1e-3)
+            out[name]["cpu_oracle"] = {
+                "steps": done, "seconds": el, "threads": threads, "value": cv, "unit": UNIT,
+                "kind": "port", "gpu_value_same_steps": gv, "gpu_over_cpu": gv / cv,
+                "sample": "steps 1..%d of the same run from its initial state" % done}
     return out
 
 
@@ -824,7 +861,7 @@ def main():
         parity = cpu_parity(args, local)
     rates = None
     if rank == 0 and world == 1 and not args.no_config_rates:
-        rates = config_rates(args, local)
+        rates = config_rates(args, local, cpu=not args.no_cpu_baseline)
         rates["fractal_inlet_%d" % n] = {"grid": [n, n], "steps": args.steps, "value": value,
                                          "unit": UNIT, "ms_per_step": ms / args.steps,
                                          "note": "the headline value (2 m initial layer)"}
