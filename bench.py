@@ -275,7 +275,9 @@ def _oracle_config_rate(p, st, q, steps, budget_s):
     import oracle as orc
     timing = orc.timing_build_usable()
     orc.build(target=orc.TIMING if timing else orc.CHECKER)
-    threads = orc.lib(orc.TIMING if timing else orc.CHECKER).oracle_max_threads()
+    # every host thread this process may run on (OpenMP's current maximum
+    # is whatever the last Oracle set, 1 after the one-thread baseline)
+    threads = len(os.sched_getaffinity(0))
     o = orc.Oracle(p, st, threads=threads, timing=timing)
     o.set_state(q, 0.0)
     o.set_clock(0.0, 1e-2)
