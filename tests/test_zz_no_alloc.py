@@ -70,3 +70,36 @@ def test_noalloc_allocates_no_device_memory():
     free1, _ = torch.cuda.mem_get_info()
     assert free1 == free0, (free0, free1)
     g.close()
+
+
+def test_noalloc_tile_limit_one_row_grids():
+    """The built-in scratch holds one slot per 32x8 tile, 1,048,576 of them.
+    A one-row grid of 32 * 1,048,576 cells needs exactly that many tiles: it
+    is accepted and gives imex_gpu_timestep's dt (the fold then reduces the
+    largest number of tile minima it takes).  One cell more needs one tile
+    more and is rejected with IMEX_EINVAL, before any launch.  Each grid is
+    a dam break along the row (33.5 M cells, about 9 GB on the device)."""
+    import numpy as np
+    from imex_sflow2d_v2_b200 import configs
+    from imex_sflow2d_v2_b200.abi import IMEX_EINVAL
+    from imex_sflow2d_v2_b200.solver import ImexError
+    limit = 1 << 20
+    for nx, fits in ((32 * limit, True), (32 * limit + 1, False)):
+        p, st, q = configs.dambreak(nx=nx, ny=1, dx=0.05, x_split=nx * 0.05 * 0.5)
+        g = ImexSolver(p, st)
+        try:
+            g.set_state(q, 0.0)
+            del q, st
+            g.check_solve(0.0)
+            d0 = g.timestep()
+            if fits:
+                assert _close(g.timestep_noalloc(), d0)
+                assert _close(g.timestep_noalloc(), d0)
+            else:
+                with pytest.raises(ImexError) as e:
+                    g.timestep_noalloc()
+                assert e.value.code == IMEX_EINVAL
+                assert "1048577 tiles" in str(e.value), str(e.value)
+            assert np.isfinite(d0) and d0 > 0.0
+        finally:
+            g.close()
