@@ -17,7 +17,8 @@ update_erosion_deposition_cell) on the device.
             step uploads q from pinned host memory, advances, and reads q back
   roofline  dominant kernel: algorithmic bytes per launch / its mean event time
   cpu_baseline  the CPU oracle (a line-by-line C++ port of the reference,
-            OpenMP) on a 512^2 instance of the same workload generator
+            OpenMP) on the same 4096^2 workload with all host threads (a
+            512^2 instance of the generator with one thread)
 
 `--impl reference` times that CPU port alone (the reference itself is
 Fortran and cannot be built here: no Fortran compiler in the image).
@@ -49,7 +50,14 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=4096, help="grid side")
     ap.add_argument("--layer", type=float, default=2.0, help="initial current thickness (m)")
-    ap.add_argument("--cpu-n", type=int, default=512, help="side of the CPU baseline sample")
+    ap.add_argument("--cpu-n", type=int, default=0,
+                    help="grid side of the all-thread CPU baseline (0 = the --n grid)")
+    ap.add_argument("--cpu1-n", type=int, default=512,
+                    help="grid side of the one-thread CPU sample")
+    ap.add_argument("--parity-n", type=int, default=512,
+                    help="grid side of the GPU-vs-oracle record")
+    ap.add_argument("--ref-budget", type=float, default=150.0,
+                    help="seconds of timed steps in --impl reference (at least one step)")
     ap.add_argument("--cpu-steps", type=int, default=0, help="0 = choose ~10-20 s of work")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -186,50 +194,60 @@ def cpu_info():
     return {"model": model, "logical_cpus": os.cpu_count(), "flags": keep}
 
 
-def _time_oracle(args, p, st, q, threads, timing, budget_s):
-    """Cell-updates/s of the oracle on (p, st, q): one untimed step, then
-    enough steps for about `budget_s` seconds (at least one)."""
+def _time_oracle(args, p, st, q, threads, timing, budget_s, warmup=1, max_steps=50):
+    """Cell-updates/s of the oracle on (p, st, q): `warmup` untimed steps
+    (at least one: page-in, thread start-up), then enough steps for about
+    `budget_s` seconds, at least one and at most `max_steps`."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
     o = orc.Oracle(p, st, threads=threads, timing=timing)
     o.set_state(q, 0.0)
     o.set_clock(0.0, 1e-2)
     t0 = time.perf_counter()
-    o.advance(1)                       # page-in, thread start-up
-    one = time.perf_counter() - t0
-    steps = args.cpu_steps if args.cpu_steps > 0 else max(1, min(50, int(budget_s / max(one, 1e-3))))
+    o.advance(max(1, warmup))
+    one = (time.perf_counter() - t0) / max(1, warmup)
+    steps = args.cpu_steps if args.cpu_steps > 0 else \
+        max(1, min(max_steps, int(budget_s / max(one, 1e-3))))
     t0 = time.perf_counter()
     o.advance(steps)
     el = time.perf_counter() - t0
     return p.nx * p.ny * steps / el, steps, el
 
 
-def cpu_baseline(args, single_thread=True):
+def cpu_baseline(args, single_thread=True, warmup=1, budget_s=15.0, max_steps=50):
     """The oracle's timing build (-O3, x86-64-v3, contraction on, stale-read
-    instrument off; the checker build if this CPU lacks AVX2/FMA) on a
-    bounded sample of the workload: the same generator at --cpu-n, with all
-    host threads and with one.  Its OpenMP loops are the reference's
-    (assembly, erosion/deposition, reconstruction, fluxes, Newton)."""
+    instrument off; the checker build if this CPU lacks AVX2/FMA) on the
+    benchmark workload itself (--cpu-n 0: the --n grid, same generator, seed
+    and physics) with all host threads, and on a --cpu1-n instance of the
+    same generator with one thread (a full-size step would take minutes
+    there).  Its OpenMP loops are the reference's (assembly,
+    erosion/deposition, reconstruction, fluxes, Newton)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
     timing = orc.timing_build_usable()
     orc.build(target=orc.TIMING if timing else orc.CHECKER)
-    p, st, q = workload(args.cpu_n, args.layer)
-    cores = orc.lib(orc.TIMING if timing else orc.CHECKER).oracle_max_threads()
-    v_all, n_all, el_all = _time_oracle(args, p, st, q, cores, timing, 15.0)
+    n_all = args.cpu_n if args.cpu_n > 0 else args.n
+    p, st, q = workload(n_all, args.layer)
+    cores = len(os.sched_getaffinity(0))
+    v_all, s_all, el_all = _time_oracle(args, p, st, q, cores, timing, budget_s, warmup,
+                                        max_steps)
+    del p, st, q
     out = {"value": v_all, "unit": UNIT, "cores": int(cores), "kind": "port",
            "build": ("oracle timing build: g++ -O3 -march=x86-64-v3 -ffp-contract=fast, "
                      "instrument off" if timing else "oracle checker build: g++ -O2 "
                      "-ffp-contract=off (no AVX2/FMA on this CPU)"),
-           "sample": "%dx%d instance of the same generator (seed, physics, 2 m layer), "
-                     "%d steps after 1 untimed, %.1f s, OpenMP %d threads"
-                     % (args.cpu_n, args.cpu_n, n_all, el_all, cores),
-           "threads_all": {"threads": int(cores), "value": v_all, "steps": n_all,
-                           "seconds": el_all},
+           "same_config": n_all == args.n,
+           "sample": "%dx%d grid of the benchmark generator (seed, physics, 2 m layer), "
+                     "%d steps after %d untimed, %.1f s, OpenMP %d threads"
+                     % (n_all, n_all, s_all, max(1, warmup), el_all, cores),
+           "threads_all": {"threads": int(cores), "grid": [n_all, n_all], "value": v_all,
+                           "steps": s_all, "seconds": el_all},
            "cpu": cpu_info()}
     if single_thread:
-        v1, n1, el1 = _time_oracle(args, p, st, q, 1, timing, 12.0)
-        out["threads_1"] = {"threads": 1, "value": v1, "steps": n1, "seconds": el1}
+        p1, st1, q1 = workload(args.cpu1_n, args.layer)
+        v1, n1, el1 = _time_oracle(args, p1, st1, q1, 1, timing, 12.0)
+        out["threads_1"] = {"threads": 1, "grid": [args.cpu1_n, args.cpu1_n], "value": v1,
+                            "steps": n1, "seconds": el1}
     return out
 
 
@@ -241,7 +259,7 @@ def cpu_parity(args, device):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
     from imex_sflow2d_v2_b200.solver import ImexSolver
-    p, st, q = workload(args.cpu_n, args.layer)
+    p, st, q = workload(args.parity_n, args.layer)
     steps = args.parity_steps
     o = orc.Oracle(p, st, threads=orc.lib().oracle_max_threads())
     g = ImexSolver(p, st, device=device)
@@ -257,7 +275,7 @@ def cpu_parity(args, device):
     ex = all(np.array_equal(a, b) for a, b in zip(o.get_exchange(), g.get_exchange()))
     so, sg = o.stats(), g.stats()
     g.close()
-    return {"workload": "%dx%d instance of the benchmark generator" % (args.cpu_n, args.cpu_n),
+    return {"workload": "%dx%d instance of the benchmark generator" % (args.parity_n, args.parity_n),
             "steps": steps, "masks_equal": bool(masks), "q_equal": bool(np.array_equal(qo, qg)),
             "exchange_equal": bool(ex), "rel_l1": rl1, "t_equal": bool(to == tg),
             "newton_iters_equal": bool(so.newton_iters == sg.newton_iters),
@@ -619,15 +637,17 @@ def run_fast(args, p, st, q0, device, cells, g_exact):
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    cb = cpu_baseline(args, single_thread=False)
+    # W untimed steps of the benchmark workload, then up to K timed steps
+    # within --ref-budget seconds (at least one)
+    cb = cpu_baseline(args, single_thread=False, warmup=args.warmup, budget_s=args.ref_budget,
+                      max_steps=args.steps)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
             "config": {"workload": workload_name(args.n), "grid": [args.n, args.n],
                        "cells": args.n * args.n, "parallelism": "host threads (OpenMP)",
-                       "sample": "each step times a %dx%d instance of the same generator "
-                                 "(cpu_baseline.sample)" % (args.cpu_n, args.cpu_n)},
+                       "sample": cb["sample"], "steps_timed": cb["threads_all"]["steps"]},
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
